@@ -1,0 +1,144 @@
+// common.cuh: device-side layout and integer primitives shared by the decision kernels.
+//
+// Planes live in HBM with a replicated margin of M samples on every side: a plane of w x h
+// samples is stored in (w + 2M) x (h + 2M) bytes, and the margin repeats the nearest edge sample.
+// The reference reads every plane through a clamped accessor (src/gpu/intra_common.h:17-25); with
+// the margin, clamping a coordinate into [-M, size + M) gives the same sample as clamping it into
+// [0, size), so kernels read directly wherever a footprint lies inside the margin and clamp to the
+// allocated extent otherwise (which is still exact, and never leaves the allocation).
+#pragma once
+#include <cstdint>
+
+#include "celv2_decision.h"
+
+namespace celv2cu {
+
+constexpr int kLevels = CELV2_ME_LEVELS;
+constexpr int kMaxRefs = CELV2_MAX_REFS;
+constexpr int kBlocks = CELV2_SB_BLOCKS;
+constexpr int kModes = CELV2_NUM_MODES;
+constexpr int kPhases = 16;
+// Decision constants (reference src/gpu/inter_common.h:35-55,140, src/gpu/intra_common.h:32-42).
+constexpr int kMeRange = 8;
+constexpr int kMePenalty = 4;
+constexpr int kSubpelPenalty = 16;
+constexpr int kInterBits = 3;
+constexpr int kIntraInInterBits = 32;
+constexpr int kPartBits = 2;
+
+// Margin per pyramid level. The motion search reaches at most 8 * (2^(5-l) - 1) pels from a cell
+// at level l (248 at level 0, plus 3/4 pel of refinement), the superblock grid overhangs the padded
+// frame by at most 56 samples and intra edges reach 95 samples past a block: 320 >> l (at least
+// 32) covers all of it, so the clamping fallback never runs for in-range inputs.
+__host__ __device__ constexpr int level_margin(int l) { return (320 >> l) < 32 ? 32 : (320 >> l); }
+
+struct DevPlane {
+  const uint8_t* p;   // the sample (0, 0); rows of `stride` bytes; valid rows/cols [-margin, size + margin)
+  int stride, w, h, margin;
+  long long phase;    // bytes between quarter-pel phase planes (level 0 of a reference), 0: none
+};
+
+struct DevPyramid {
+  DevPlane lv[kLevels];
+};
+
+// One frame's decision work as the kernels see it (written by the host per launch).
+struct FrameJob {
+  DevPyramid cur;
+  DevPyramid ref[kMaxRefs];
+  int nrefs;
+  int pw, ph;              // padded luma size (multiple of 8)
+  int sb_cols, sb_rows;
+  int fcols[kLevels], frows[kLevels];
+  int* field[kMaxRefs][kLevels];  // packed MVs: (mvy << 16) | (mvx & 0xffff)
+  const int* intra;        // [sb][kBlocks][kModes] SATDs (blocks < 5 unused)
+  int2* inter;             // [sb][kMaxRefs][kBlocks]: (best SATD, packed MV)
+  celv2_sb_out* out;       // [sb]
+  long long lam;           // lambda_q8
+  const uint32_t* items;   // the superblock's (block, tile) work items (tables.h)
+};
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// The clamped sample (Plane::at, src/gpu/intra_common.h:17-21).
+__device__ __forceinline__ int at(const DevPlane& s, int y, int x) {
+  y = clampi(y, -s.margin, s.h + s.margin - 1);
+  x = clampi(x, -s.margin, s.w + s.margin - 1);
+  return s.p[(long long)y * s.stride + x];
+}
+
+// Quarter-pel sample (Plane::at_q, src/gpu/intra_common.h:23-25): phase (qy & 3) * 4 + (qx & 3) at
+// the whole-pel position (y + (qy >> 2), x + (qx >> 2)).
+__device__ __forceinline__ int at_q(const DevPlane& s, int y, int x, int qy, int qx) {
+  const uint8_t* base = s.p + (long long)((qy & 3) * 4 + (qx & 3)) * s.phase;
+  const int yy = clampi(y + (qy >> 2), -s.margin, s.h + s.margin - 1);
+  const int xx = clampi(x + (qx >> 2), -s.margin, s.w + s.margin - 1);
+  return base[(long long)yy * s.stride + xx];
+}
+
+// Whether the rectangle [x, x + w) x [y, y + h) lies inside the stored plane (margin included).
+__device__ __forceinline__ bool inside(const DevPlane& s, int x, int y, int w, int h) {
+  return x >= -s.margin && y >= -s.margin && x + w <= s.w + s.margin && y + h <= s.h + s.margin;
+}
+
+// Four bytes starting at an arbitrary byte address, from two aligned 32-bit loads.
+__device__ __forceinline__ uint32_t load4(const uint8_t* p) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = (uint32_t)(a & 3) * 8;
+  const uint32_t lo = __ldg(w);
+  if (sh == 0) return lo;
+  return __funnelshift_r(lo, __ldg(w + 1), sh);
+}
+
+// Sum of absolute 4x4 Hadamard coefficients (src/gpu/intra_common.h:131-146): rows, then columns.
+__device__ __forceinline__ int hadamard4x4(int d[16]) {
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const int s01 = d[4 * r] + d[4 * r + 1], d01 = d[4 * r] - d[4 * r + 1];
+    const int s23 = d[4 * r + 2] + d[4 * r + 3], d23 = d[4 * r + 2] - d[4 * r + 3];
+    d[4 * r] = s01 + s23, d[4 * r + 1] = d01 + d23, d[4 * r + 2] = s01 - s23, d[4 * r + 3] = d01 - d23;
+  }
+  int sum = 0;
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const int s01 = d[c] + d[4 + c], d01 = d[c] - d[4 + c];
+    const int s23 = d[8 + c] + d[12 + c], d23 = d[8 + c] - d[12 + c];
+    sum += abs(s01 + s23) + abs(d01 + d23) + abs(s01 - s23) + abs(d01 - d23);
+  }
+  return sum;
+}
+
+// Residual of one 4x4 row: four cur bytes minus four prediction bytes.
+__device__ __forceinline__ void residual_row(int* d, uint32_t c, uint32_t p) {
+  d[0] = (int)(c & 255) - (int)(p & 255);
+  d[1] = (int)((c >> 8) & 255) - (int)((p >> 8) & 255);
+  d[2] = (int)((c >> 16) & 255) - (int)((p >> 16) & 255);
+  d[3] = (int)(c >> 24) - (int)(p >> 24);
+}
+
+__device__ __forceinline__ int mv_x(int packed) { return (int)(short)(packed & 0xffff); }
+__device__ __forceinline__ int mv_y(int packed) { return packed >> 16; }
+__host__ __device__ __forceinline__ int pack_mv(int x, int y) { return (int)(((unsigned)y << 16) | ((unsigned)x & 0xffffu)); }
+
+// ---- Superblock block geometry (src/gpu/sb_blocks.h:12-37) ----
+__host__ __device__ __forceinline__ int sb_level_offset(int level) { return ((1 << (2 * level)) - 1) / 3; }
+
+__host__ __device__ __forceinline__ void sb_block_geom(int b, int& x, int& y, int& w, int& h) {
+  const int sq = b / 5, kind = b % 5;
+  const int level = sq >= 21 ? 3 : sq >= 5 ? 2 : sq >= 1 ? 1 : 0;
+  const int idx = sq - sb_level_offset(level), n = 1 << level, size = 64 >> level, half = size / 2;
+  const int sx = (idx % n) * size, sy = (idx / n) * size;
+  x = sx, y = sy, w = size, h = size;
+  if (kind == 1 || kind == 2) h = half, y = sy + (kind == 2 ? half : 0);
+  if (kind == 3 || kind == 4) w = half, x = sx + (kind == 4 ? half : 0);
+}
+
+__host__ __device__ __forceinline__ int mode_bits(int mode) { return mode == 0 ? 1 : mode < 4 ? 3 : 9; }
+
+__host__ __device__ __forceinline__ bool compound_pair_ok(int a, int b, int nrefs) {
+  const int lo = a < b ? a : b, limit = nrefs - 2 < 2 ? nrefs - 2 : 2;
+  return a != b && lo <= limit;
+}
+
+}  // namespace celv2cu

@@ -1,0 +1,742 @@
+// engine.cu: the host side of the B200 decision engine behind the C ABI of include/celv2_cuda.h.
+//
+// Structure (per engine, one resolution, one GPU):
+//  - a frame store in HBM: keyed slots holding a frame's 5-level pyramid with replicated margins
+//    and, for references, the 15 quarter-pel phase planes (the reference Vulkan engine's RefSlot,
+//    src/vk/vk_engine.cpp:71-78,239-258: the slot of a key is reused, else one this launch does not
+//    need, else a new one);
+//  - two source slots: while one frame is decided, prepare() builds the next one's pyramid and
+//    intra SATDs on a second stream (vk_engine.cpp:80-87,188-205);
+//  - per launch: the stage kernels on the main stream -- motion search level by level for every
+//    reference, intra (unless prepared), inter candidates, finalize -- then one device-to-host
+//    copy per superblock row with an event, so rows are collected as they arrive
+//    (vk_engine.cpp:288-328);
+//  - uploads go through a ring of pinned staging buffers: launch() copies the caller's planes into
+//    pinned memory before it returns (the reference requires that the inputs may change at once,
+//    decision_engine.h:12-16).
+// No CPU fallback: every decision is made by the kernels; a missing GPU is an error.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "celv2_cuda.h"
+#include "kernels.h"
+#include "tables.h"
+
+namespace celv2cu {
+cudaError_t inter_attributes();
+cudaError_t intra_attributes();
+cudaError_t finalize_attributes();
+}  // namespace celv2cu
+
+using namespace celv2cu;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw Error(CELV2_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(x) check((x), #x)
+
+void invalid(const std::string& m) { throw Error(CELV2_EINVAL, m); }
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return CELV2_OK;
+  } catch (const Error& e) {
+    g_error = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return CELV2_ECUDA;
+  }
+}
+
+std::mutex g_init_mu;
+std::vector<uint32_t*> g_items;  // per device: the (block, tile) item table, made once
+
+const uint32_t* init_device(int dev) {
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  if ((int)g_items.size() <= dev) g_items.resize(dev + 1, nullptr);
+  if (g_items[dev]) return g_items[dev];
+  CK(inter_attributes());
+  CK(intra_attributes());
+  CK(finalize_attributes());
+  uint32_t* items = nullptr;
+  CK(make_items(&items));
+  g_items[dev] = items;
+  return items;
+}
+
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Geometry of one frame size: padded luma, pyramid levels, fields, superblocks.
+struct Geometry {
+  int width = 0, height = 0, pw = 0, ph = 0;
+  int w[kLevels], h[kLevels], margin[kLevels], stride[kLevels];
+  size_t level_bytes[kLevels], level_off[kLevels];
+  size_t pyr_bytes = 0, pyr_bytes_phases = 0;
+  int fcols[kLevels], frows[kLevels];
+  int sb_cols = 0, sb_rows = 0, nsb = 0;
+  size_t field_ints = 0;  // all levels of one reference
+
+  void set(int width_, int height_) {
+    width = width_, height = height_;
+    pw = (width + 7) & ~7, ph = (height + 7) & ~7;
+    for (int l = 0; l < kLevels; l++) {
+      w[l] = l ? w[l - 1] / 2 : pw;
+      h[l] = l ? h[l - 1] / 2 : ph;
+      margin[l] = level_margin(l);
+      stride[l] = (int)align_up((size_t)w[l] + 2 * margin[l], 64);
+      level_bytes[l] = align_up((size_t)stride[l] * (h[l] + 2 * margin[l]), 256);
+      fcols[l] = (w[l] + 7) / 8, frows[l] = (h[l] + 7) / 8;
+    }
+    // level 0 first (its 15 phases follow it when present), then levels 1-4
+    size_t off = 0;
+    level_off[0] = 0;
+    off = level_bytes[0];
+    for (int l = 1; l < kLevels; l++) level_off[l] = off, off += level_bytes[l];
+    pyr_bytes = off;
+    pyr_bytes_phases = off + (kPhases - 1) * level_bytes[0];
+    sb_cols = (width + 63) / 64, sb_rows = (height + 63) / 64, nsb = sb_cols * sb_rows;
+    field_ints = 0;
+    for (int l = 0; l < kLevels; l++) field_ints += (size_t)fcols[l] * frows[l];
+  }
+};
+
+// A frame's pyramid in HBM.
+struct Slot {
+  long long key = -1;
+  long long used = -1;
+  bool phases = false;
+  uint8_t* mem = nullptr;
+  size_t bytes = 0;
+  DevPyramid pyr{};
+};
+
+// One pinned staging buffer with its device copy (an upload in flight).
+struct Stage {
+  void* host = nullptr;
+  void* dev = nullptr;
+  size_t bytes = 0;
+  cudaEvent_t done = nullptr;
+  bool pending = false;
+};
+
+// Per-frame device buffers of a decision.
+struct JobBuffers {
+  int* fields = nullptr;     // kMaxRefs * field_ints
+  int* intra = nullptr;      // nsb * kBlocks * kModes
+  int2* inter = nullptr;     // nsb * kMaxRefs * kBlocks
+  celv2_sb_out* out = nullptr;
+};
+
+}  // namespace
+
+struct celv2_engine {
+  int device = 0;
+  Geometry g;
+  const uint32_t* items = nullptr;
+  cudaStream_t st = nullptr, prep_st = nullptr;
+  cudaEvent_t prep_done = nullptr;
+  std::vector<Slot*> store;      // keyed frames (references, resident frames)
+  Slot srcs[2];                  // sources of launch / prepare
+  int cur_src = 0;
+  long long launches = 0;
+  std::vector<Stage> stages;
+  int next_stage = 0;
+  JobBuffers single;             // the launch() path
+  int* intra_prep[2] = {nullptr, nullptr};  // intra SATDs per source slot
+  celv2_sb_out* host_out = nullptr;          // pinned, nsb records
+  std::vector<cudaEvent_t> row_done;
+  std::vector<int> order;
+  int row_streams = 1;
+  bool pending = false;
+  int last_nrefs = 0;
+  FrameJob* djobs = nullptr;     // 2 * kMaxJobs + 1 device descriptors (the last: prepare's)
+  // Descriptors go to the device from a ring of pinned buffers: an asynchronous copy from pageable
+  // memory may wait for the stream, which would serialise back-to-back launches.
+  static constexpr int kRing = 8, kRingJobs = 2 * kMaxJobs + 1;
+  FrameJob* ring = nullptr;
+  cudaEvent_t ring_done[kRing] = {};
+  bool ring_pending[kRing] = {};
+  int ring_next = 0;
+  // group path
+  int group_cap = 0;
+  std::vector<JobBuffers> group;
+  celv2_sb_out* group_host = nullptr;
+  int group_jobs = 0;
+  long long kernel_launches = 0;
+
+  ~celv2_engine() {
+    cudaSetDevice(device);
+    if (st) cudaStreamSynchronize(st);
+    if (prep_st) cudaStreamSynchronize(prep_st);
+    for (Slot* s : store) cudaFree(s->mem), delete s;
+    for (Slot& s : srcs) cudaFree(s.mem);
+    for (Stage& s : stages) {
+      cudaFreeHost(s.host), cudaFree(s.dev);
+      if (s.done) cudaEventDestroy(s.done);
+    }
+    free_buffers(single);
+    for (JobBuffers& b : group) free_buffers(b);
+    for (int* p : intra_prep) cudaFree(p);
+    cudaFreeHost(host_out);
+    cudaFreeHost(group_host);
+    for (cudaEvent_t e : row_done) cudaEventDestroy(e);
+    cudaFree(djobs);
+    cudaFreeHost(ring);
+    for (cudaEvent_t e : ring_done)
+      if (e) cudaEventDestroy(e);
+    if (prep_done) cudaEventDestroy(prep_done);
+    if (st) cudaStreamDestroy(st);
+    if (prep_st) cudaStreamDestroy(prep_st);
+  }
+
+  static void free_buffers(JobBuffers& b) {
+    cudaFree(b.fields), cudaFree(b.intra), cudaFree(b.inter), cudaFree(b.out);
+    b = JobBuffers{};
+  }
+
+  void alloc_buffers(JobBuffers& b, bool with_intra) {
+    CK(cudaMalloc(&b.fields, kMaxRefs * g.field_ints * sizeof(int)));
+    if (with_intra) CK(cudaMalloc(&b.intra, (size_t)g.nsb * kBlocks * kModes * sizeof(int)));
+    CK(cudaMalloc(&b.inter, (size_t)g.nsb * kMaxRefs * kBlocks * sizeof(int2)));
+    CK(cudaMalloc(&b.out, (size_t)g.nsb * sizeof(celv2_sb_out)));
+  }
+
+  void init(int width, int height, int dev) {
+    device = dev;
+    CK(cudaSetDevice(dev));
+    items = init_device(dev);
+    g.set(width, height);
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&prep_st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&prep_done, cudaEventDisableTiming));
+    CK(cudaMalloc(&djobs, kRingJobs * sizeof(FrameJob)));
+    CK(cudaMallocHost(&ring, (size_t)kRing * kRingJobs * sizeof(FrameJob)));
+    for (cudaEvent_t& e : ring_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    alloc_buffers(single, false);
+    for (int*& p : intra_prep) CK(cudaMalloc(&p, (size_t)g.nsb * kBlocks * kModes * sizeof(int)));
+    CK(cudaMallocHost(&host_out, (size_t)g.nsb * sizeof(celv2_sb_out)));
+    row_done.resize(g.sb_rows);
+    for (cudaEvent_t& e : row_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    stages.resize(16);
+    for (Stage& s : stages) CK(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+    for (Slot& s : srcs) alloc_slot(s, false);
+  }
+
+  // ---- frame pyramids ----
+  void alloc_slot(Slot& s, bool phases) {
+    // + slack: an unaligned 4-byte read (load4) may touch up to 3 bytes past the last row
+    const size_t need = (phases ? g.pyr_bytes_phases : g.pyr_bytes) + 256;
+    if (s.mem && s.bytes >= need) return;
+    if (s.mem) CK(cudaFree(s.mem));
+    s.mem = nullptr;
+    CK(cudaMalloc(&s.mem, need));
+    s.bytes = need;
+    for (int l = 0; l < kLevels; l++) {
+      DevPlane& p = s.pyr.lv[l];
+      // level 0's phases sit right after it: levels 1-4 move behind the phases
+      const size_t off = l == 0 ? 0 : (phases ? g.level_off[l] + (kPhases - 1) * g.level_bytes[0] : g.level_off[l]);
+      p.p = s.mem + off + (size_t)g.margin[l] * g.stride[l] + g.margin[l];
+      p.stride = g.stride[l], p.w = g.w[l], p.h = g.h[l], p.margin = g.margin[l];
+      p.phase = l == 0 && phases ? (long long)g.level_bytes[0] : 0;
+    }
+    s.phases = false;
+  }
+
+  Stage& take_stage(size_t bytes) {
+    Stage& s = stages[next_stage];
+    next_stage = (next_stage + 1) % (int)stages.size();
+    if (s.pending) CK(cudaEventSynchronize(s.done)), s.pending = false;
+    if (s.bytes < bytes) {
+      if (s.host) CK(cudaFreeHost(s.host));
+      if (s.dev) CK(cudaFree(s.dev));
+      s.host = s.dev = nullptr;
+      CK(cudaMallocHost(&s.host, bytes));
+      CK(cudaMalloc(&s.dev, bytes));
+      s.bytes = bytes;
+    }
+    return s;
+  }
+
+  void check_frame(const celv2_frame* f, const char* what) {
+    if (!f) invalid(std::string(what) + ": null frame");
+    if (f->width != g.width || f->height != g.height)
+      invalid(std::string("CudaEngine: ") + what + " size does not match the engine");
+    if (!f->y && !f->hy) invalid(std::string(what) + ": no luma plane");
+    if (!f->y && (f->bit_depth < 9 || f->bit_depth > 16)) invalid(std::string(what) + ": bit depth must be 9..16");
+    if (f->pitch && f->pitch < g.pw) invalid(std::string(what) + ": pitch below the padded width");
+  }
+
+  // Copies f's luma into pinned memory (synchronously: the caller may change it afterwards), then
+  // queues its upload, the 8-bit level 0, the pyramid and (phases) the quarter-pel planes.
+  void upload(const celv2_frame* f, Slot& s, bool phases, cudaStream_t stream) {
+    alloc_slot(s, phases || s.phases);
+    const bool wide = f->y == nullptr;
+    const int pitch = f->pitch ? f->pitch : g.pw;
+    const size_t row = (size_t)g.pw * (wide ? 2 : 1);
+    Stage& sg = take_stage(row * g.ph);
+    const uint8_t* src = wide ? reinterpret_cast<const uint8_t*>(f->hy) : f->y;
+    const size_t spitch = (size_t)pitch * (wide ? 2 : 1);
+    if (spitch == row) {
+      std::memcpy(sg.host, src, row * g.ph);
+    } else {
+      for (int r = 0; r < g.ph; r++) std::memcpy((uint8_t*)sg.host + r * row, src + r * spitch, row);
+    }
+    CK(cudaMemcpyAsync(sg.dev, sg.host, row * g.ph, cudaMemcpyHostToDevice, stream));
+    if (wide)
+      launch_expand_u16((const uint16_t*)sg.dev, g.pw, f->bit_depth, s.pyr.lv[0], stream);
+    else
+      launch_expand_u8((const uint8_t*)sg.dev, g.pw, s.pyr.lv[0], stream);
+    CK(cudaEventRecord(sg.done, stream));
+    sg.pending = true;
+    launch_pyramid(s.pyr, stream);
+    kernel_launches += 1 + (kLevels - 1);
+    s.phases = false;
+    if (phases) make_phases(s, stream);
+  }
+
+  void make_phases(Slot& s, cudaStream_t stream) {
+    if (s.phases) return;
+    launch_phases(s.pyr.lv[0], stream);
+    kernel_launches++;
+    s.phases = true;
+  }
+
+  // The store's slot for `key` (keys of this launch are protected), else a free or new one.
+  Slot* ref_slot(long long key, const long long* keys, int nkeys, long long now, bool& fresh) {
+    fresh = false;
+    if (key >= 0)
+      for (Slot* s : store)
+        if (s->key == key) return s;
+    Slot* pick = nullptr;
+    for (Slot* s : store) {
+      if (s->used == now) continue;
+      bool needed = false;
+      for (int i = 0; i < nkeys && keys; i++) needed |= s->key >= 0 && s->key == keys[i];
+      if (needed) continue;
+      if (!pick || s->used < pick->used) pick = s;
+    }
+    if (!pick) {
+      pick = new Slot;
+      store.push_back(pick);
+    }
+    pick->key = -1;
+    fresh = true;
+    return pick;
+  }
+
+  void fill_job(FrameJob& job, const DevPyramid& cur, Slot* const* refs, int nrefs, const JobBuffers& b,
+                const int* intra, long long lam) {
+    std::memset(&job, 0, sizeof job);
+    job.cur = cur;
+    for (int r = 0; r < nrefs; r++) job.ref[r] = refs[r]->pyr;
+    job.nrefs = nrefs;
+    job.pw = g.pw, job.ph = g.ph;
+    job.sb_cols = g.sb_cols, job.sb_rows = g.sb_rows;
+    for (int l = 0; l < kLevels; l++) job.fcols[l] = g.fcols[l], job.frows[l] = g.frows[l];
+    for (int r = 0; r < kMaxRefs; r++) {
+      size_t off = r * g.field_ints;
+      for (int l = 0; l < kLevels; l++) {
+        job.field[r][l] = b.fields + off;
+        off += (size_t)g.fcols[l] * g.frows[l];
+      }
+    }
+    job.intra = intra;
+    job.inter = b.inter;
+    job.out = b.out;
+    job.lam = lam;
+    job.items = items;
+  }
+
+  // Queues the copy of n descriptors to dst (device) through the pinned ring.
+  void put_jobs(const FrameJob* jobs, int n, FrameJob* dst, cudaStream_t stream) {
+    const int i = ring_next;
+    ring_next = (ring_next + 1) % kRing;
+    if (ring_pending[i]) CK(cudaEventSynchronize(ring_done[i])), ring_pending[i] = false;
+    FrameJob* h = ring + (size_t)i * kRingJobs;
+    std::memcpy(h, jobs, n * sizeof(FrameJob));
+    CK(cudaMemcpyAsync(dst, h, n * sizeof(FrameJob), cudaMemcpyHostToDevice, stream));
+    CK(cudaEventRecord(ring_done[i], stream));
+    ring_pending[i] = true;
+  }
+
+  // The stage kernels of the jobs; intra for the jobs flagged.
+  void run_stages(const std::vector<FrameJob>& jobs, const std::vector<char>& need_intra, cudaStream_t stream) {
+    const int n = (int)jobs.size();
+    put_jobs(jobs.data(), n, djobs, stream);
+    WorkList w{};
+    w.njobs = n;
+    for (int l = kLevels - 1; l >= 0; l--) {
+      for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].nrefs * jobs[j].fcols[l] * jobs[j].frows[l];
+      if (w.prefix[n] > 0) launch_me_level(djobs, w, l, stream), kernel_launches++;
+    }
+    for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + (need_intra[j] ? jobs[j].sb_cols * jobs[j].sb_rows : 0);
+    if (w.prefix[n] > 0) {
+      // only the flagged jobs: a list of them with their own prefix
+      std::vector<FrameJob> sub;
+      for (int j = 0; j < n; j++)
+        if (need_intra[j]) sub.push_back(jobs[j]);
+      if ((int)sub.size() == n) {
+        launch_intra(djobs, w, stream);
+      } else {
+        // the flagged jobs' descriptors go after the batch's
+        put_jobs(sub.data(), (int)sub.size(), djobs + n, stream);
+        WorkList ws{};
+        ws.njobs = (int)sub.size();
+        for (int j = 0; j < ws.njobs; j++) ws.prefix[j + 1] = ws.prefix[j] + sub[j].sb_cols * sub[j].sb_rows;
+        launch_intra(djobs + n, ws, stream);
+      }
+      kernel_launches++;
+    }
+    for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].nrefs * jobs[j].sb_cols * jobs[j].sb_rows;
+    if (w.prefix[n] > 0) launch_inter(djobs, w, stream), kernel_launches++;
+    for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].sb_cols * jobs[j].sb_rows;
+    launch_finalize(djobs, w, stream);
+    kernel_launches++;
+    CK(cudaGetLastError());
+  }
+
+  void wait_idle() {
+    CK(cudaStreamSynchronize(st));
+    pending = false;
+  }
+
+  void launch(const celv2_frame* src, const celv2_frame* refs, int nrefs, long long lam, const long long* keys,
+              long long src_key) {
+    check_frame(src, "source");
+    if (nrefs < 0 || nrefs > kMaxRefs) invalid("CudaEngine: too many references");
+    for (int r = 0; r < nrefs; r++) check_frame(&refs[r], "reference");
+    if (nrefs > 0 && (g.pw < 16 || g.ph < 16)) invalid("CudaEngine: inter frames need at least 9x9 pixels");
+    if (pending) wait_idle();
+    try {
+      // the prepared source, else an upload into the other slot
+      int use = -1;
+      for (int i = 0; i < 2; i++)
+        if (src_key >= 0 && srcs[i].key == src_key) use = i;
+      const bool prepared = use >= 0;
+      if (prepared) {
+        CK(cudaStreamWaitEvent(st, prep_done, 0));
+      } else {
+        use = 1 - cur_src;
+        CK(cudaStreamSynchronize(prep_st));  // a prepare() into this slot may still run
+        upload(src, srcs[use], false, st);
+      }
+      srcs[use].key = -1;  // used: a later prepare() may overwrite it
+      cur_src = use;
+      const long long now = ++launches;
+      Slot* used[kMaxRefs];
+      for (int r = 0; r < nrefs; r++) {
+        bool fresh;
+        Slot* s = ref_slot(keys ? keys[r] : -1, keys, keys ? nrefs : 0, now, fresh);
+        if (fresh) {
+          upload(&refs[r], *s, true, st);
+          s->key = keys ? keys[r] : -1;
+        } else {
+          make_phases(*s, st);
+        }
+        s->used = now;
+        used[r] = s;
+      }
+      std::vector<FrameJob> jobs(1);
+      fill_job(jobs[0], srcs[use].pyr, used, nrefs, single, intra_prep[use], lam);
+      run_stages(jobs, std::vector<char>{static_cast<char>(!prepared)}, st);
+      last_nrefs = nrefs;
+      // rows back to the host in row-stream order
+      const int streams = std::max(1, std::min(row_streams, g.sb_rows));
+      const int run = (g.sb_rows + streams - 1) / streams;
+      order.clear();
+      for (int i = 0; i < run; i++)
+        for (int s = 0; s < streams; s++)
+          if (s * run + i < g.sb_rows) order.push_back(s * run + i);
+      for (int r : order) {
+        const size_t first = (size_t)r * g.sb_cols;
+        CK(cudaMemcpyAsync(host_out + first, single.out + first, g.sb_cols * sizeof(celv2_sb_out),
+                           cudaMemcpyDeviceToHost, st));
+        CK(cudaEventRecord(row_done[r], st));
+      }
+      pending = true;
+    } catch (...) {
+      cudaStreamSynchronize(st);  // a failure leaves no work running
+      cudaStreamSynchronize(prep_st);
+      pending = false;
+      throw;
+    }
+  }
+
+  void prepare(const celv2_frame* next, long long key) {
+    if (key < 0 || !next || next->width != g.width || next->height != g.height) return;
+    check_frame(next, "next frame");
+    Slot& s = srcs[1 - cur_src];
+    s.key = -1;
+    // the slot's previous use (two launches back) was collected; the current launch uses the other
+    upload(next, s, false, prep_st);
+    std::vector<FrameJob> jobs(1);
+    JobBuffers none{};
+    fill_job(jobs[0], s.pyr, nullptr, 0, none, intra_prep[1 - cur_src], 0);
+    // the intra stage alone, from a descriptor area of its own (the main stream owns djobs[0..])
+    FrameJob* dprep = djobs + kRingJobs - 1;
+    put_jobs(jobs.data(), 1, dprep, prep_st);
+    WorkList w{};
+    w.njobs = 1;
+    w.prefix[1] = g.nsb;
+    launch_intra(dprep, w, prep_st);
+    kernel_launches++;
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(prep_done, prep_st));
+    s.key = key;
+  }
+
+  const celv2_sb_out* wait_row(int row) {
+    if (row < 0 || row >= g.sb_rows) invalid("row out of range");
+    if (!pending && launches == 0) throw Error(CELV2_ESTATE, "no launch to collect");
+    CK(cudaEventSynchronize(row_done[row]));
+    return host_out + (size_t)row * g.sb_cols;
+  }
+
+  // ---- group path ----
+  void reserve_group(int frames) {
+    if (frames <= group_cap) return;
+    wait_idle();
+    for (JobBuffers& b : group) free_buffers(b);
+    group.assign(frames, JobBuffers{});
+    for (JobBuffers& b : group) alloc_buffers(b, true);
+    if (group_host) CK(cudaFreeHost(group_host));
+    CK(cudaMallocHost(&group_host, (size_t)frames * g.nsb * sizeof(celv2_sb_out)));
+    group_cap = frames;
+  }
+
+  Slot* find(long long key) {
+    for (Slot* s : store)
+      if (key >= 0 && s->key == key) return s;
+    return nullptr;
+  }
+
+  void upload_store(const celv2_frame* f, long long key) {
+    check_frame(f, "frame");
+    if (key < 0) invalid("store keys must be >= 0");
+    if (pending) wait_idle();
+    Slot* s = find(key);
+    if (!s) {
+      s = new Slot;
+      store.push_back(s);
+    }
+    s->key = -1;
+    upload(f, *s, true, st);
+    s->key = key;
+    s->used = launches;
+  }
+
+  void launch_group(int njobs, const long long* src_keys, const int* nrefs, const long long* const* ref_keys,
+                    const int64_t* lams, bool to_host) {
+    if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per group");
+    if (njobs > group_cap) reserve_group(std::max(njobs, 8));
+    std::vector<FrameJob> jobs(njobs);
+    for (int j = 0; j < njobs; j++) {
+      Slot* cur = find(src_keys[j]);
+      if (!cur) invalid("group: no stored frame with the source key");
+      if (nrefs[j] < 0 || nrefs[j] > kMaxRefs) invalid("group: too many references");
+      if (nrefs[j] > 0 && (g.pw < 16 || g.ph < 16)) invalid("group: inter frames need at least 9x9 pixels");
+      Slot* refs[kMaxRefs];
+      for (int r = 0; r < nrefs[j]; r++) {
+        refs[r] = find(ref_keys[j][r]);
+        if (!refs[r]) invalid("group: no stored frame with a reference key");
+        make_phases(*refs[r], st);
+      }
+      fill_job(jobs[j], cur->pyr, refs, nrefs[j], group[j], group[j].intra, lams[j]);
+    }
+    run_stages(jobs, std::vector<char>(njobs, 1), st);
+    if (to_host)
+      for (int j = 0; j < njobs; j++)
+        CK(cudaMemcpyAsync(group_host + (size_t)j * g.nsb, group[j].out, g.nsb * sizeof(celv2_sb_out),
+                           cudaMemcpyDeviceToHost, st));
+    group_jobs = njobs;
+    ++launches;
+    pending = true;
+  }
+};
+
+extern "C" {
+
+const char* celv2_last_error(void) { return g_error.c_str(); }
+
+int celv2_create(int width, int height, int sb_size, int device, celv2_engine** out) {
+  if (out) *out = nullptr;
+  return guarded([&] {
+    if (!out) invalid("null output pointer");
+    if (width <= 0 || height <= 0) invalid("CudaEngine: frame size must be positive");
+    if (sb_size != 64) invalid("CudaEngine: only 64x64 superblocks are supported");
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) invalid("CudaEngine: no such CUDA device");
+    auto* e = new celv2_engine;
+    try {
+      e->init(width, height, device);
+    } catch (...) {
+      delete e;
+      throw;
+    }
+    *out = e;
+  });
+}
+
+void celv2_destroy(celv2_engine* e) { delete e; }
+
+int celv2_launch(celv2_engine* e, const celv2_frame* src, const celv2_frame* refs, int nrefs, int64_t lambda_q8,
+                 const long long* ref_keys, long long src_key) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    CK(cudaSetDevice(e->device));
+    if (nrefs > 0 && !refs) invalid("null references");
+    e->launch(src, refs, nrefs, lambda_q8, ref_keys, src_key);
+  });
+}
+
+int celv2_prepare(celv2_engine* e, const celv2_frame* next, long long key) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    CK(cudaSetDevice(e->device));
+    e->prepare(next, key);
+  });
+}
+
+int celv2_set_row_streams(celv2_engine* e, int n) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    e->row_streams = n < 1 ? 1 : n;
+  });
+}
+
+int celv2_geometry(const celv2_engine* e, int* sb_cols, int* sb_rows) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    if (sb_cols) *sb_cols = e->g.sb_cols;
+    if (sb_rows) *sb_rows = e->g.sb_rows;
+  });
+}
+
+int celv2_row_order(const celv2_engine* e, int* rows) {
+  return guarded([&] {
+    if (!e || !rows) invalid("null argument");
+    if (e->order.empty()) throw Error(CELV2_ESTATE, "no launch yet");
+    std::copy(e->order.begin(), e->order.end(), rows);
+  });
+}
+
+int celv2_wait_row(celv2_engine* e, int row, const celv2_sb_out** records) {
+  return guarded([&] {
+    if (!e || !records) invalid("null argument");
+    CK(cudaSetDevice(e->device));
+    *records = e->wait_row(row);
+  });
+}
+
+int celv2_finish(celv2_engine* e) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    CK(cudaStreamSynchronize(e->prep_st));
+  });
+}
+
+int celv2_upload(celv2_engine* e, const celv2_frame* f, long long key) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    CK(cudaSetDevice(e->device));
+    e->upload_store(f, key);
+  });
+}
+
+int celv2_launch_group(celv2_engine* e, int njobs, const long long* src_keys, const int* nrefs,
+                       const long long* const* ref_keys, const int64_t* lambda_q8, int to_host) {
+  return guarded([&] {
+    if (!e || !src_keys || !nrefs || !lambda_q8) invalid("null argument");
+    CK(cudaSetDevice(e->device));
+    e->launch_group(njobs, src_keys, nrefs, ref_keys, lambda_q8, to_host != 0);
+  });
+}
+
+int celv2_reserve_group(celv2_engine* e, int frames) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    if (frames < 1 || frames > kMaxJobs - 1) invalid("1..31 frames per group");
+    CK(cudaSetDevice(e->device));
+    e->reserve_group(frames);
+  });
+}
+
+int celv2_group_records(celv2_engine* e, int job, const celv2_sb_out** records) {
+  return guarded([&] {
+    if (!e || !records) invalid("null argument");
+    if (job < 0 || job >= e->group_jobs) invalid("no such job in the last group");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    *records = e->group_host + (size_t)job * e->g.nsb;
+  });
+}
+
+int celv2_clear_store(celv2_engine* e) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    for (Slot* s : e->store) cudaFree(s->mem), delete s;
+    e->store.clear();
+  });
+}
+
+int celv2_debug_field(celv2_engine* e, int r, int level, int32_t* out, int* cols, int* rows) {
+  return guarded([&] {
+    if (!e || !out) invalid("null argument");
+    if (r < 0 || r >= kMaxRefs || level < 0 || level >= kLevels) invalid("bad reference or level");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    size_t off = r * e->g.field_ints;
+    for (int l = 0; l < level; l++) off += (size_t)e->g.fcols[l] * e->g.frows[l];
+    const size_t n = (size_t)e->g.fcols[level] * e->g.frows[level];
+    CK(cudaMemcpy(out, e->single.fields + off, n * sizeof(int), cudaMemcpyDeviceToHost));
+    if (cols) *cols = e->g.fcols[level];
+    if (rows) *rows = e->g.frows[level];
+  });
+}
+
+int celv2_debug_intra(celv2_engine* e, int32_t* out) {
+  return guarded([&] {
+    if (!e || !out) invalid("null argument");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    CK(cudaMemcpy(out, e->intra_prep[e->cur_src], (size_t)e->g.nsb * kBlocks * kModes * sizeof(int),
+                  cudaMemcpyDeviceToHost));
+  });
+}
+
+int celv2_debug_inter(celv2_engine* e, int32_t* out) {
+  return guarded([&] {
+    if (!e || !out) invalid("null argument");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    CK(cudaMemcpy(out, e->single.inter, (size_t)e->g.nsb * kMaxRefs * kBlocks * sizeof(int2), cudaMemcpyDeviceToHost));
+  });
+}
+
+long long celv2_kernel_launches(const celv2_engine* e) { return e ? e->kernel_launches : 0; }
+
+}  // extern "C"

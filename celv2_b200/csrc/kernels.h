@@ -1,0 +1,49 @@
+// kernels.h: host-side launchers of the decision engine's CUDA stages.
+//
+// Every stage takes a list of frame jobs (FrameJob, device memory) so one launch scores several
+// frames -- the leaf B frames of a mini-GOP, or frames of several streams of different sizes --
+// and each CTA finds its job and unit from a prefix table of the jobs' unit counts.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace celv2cu {
+
+constexpr int kMaxJobs = 32;
+
+// Units of one stage per job, as prefix sums: job j owns units [prefix[j], prefix[j + 1]).
+struct WorkList {
+  int njobs;
+  int prefix[kMaxJobs + 1];
+};
+
+// Unit u's job (a linear scan: at most kMaxJobs jobs).
+__device__ __forceinline__ int job_of(const WorkList& w, int u) {
+  int j = 0;
+  while (j + 1 < w.njobs && u >= w.prefix[j + 1]) j++;
+  return j;
+}
+
+void launch_expand_u8(const uint8_t* raw, int pitch, const DevPlane& lv0, cudaStream_t st);
+void launch_expand_u16(const uint16_t* raw, int pitch, int bit_depth, const DevPlane& lv0, cudaStream_t st);
+void launch_pyramid(const DevPyramid& pyr, cudaStream_t st);
+void launch_phases(const DevPlane& lv0, cudaStream_t st);
+
+// Motion search of one pyramid level for every (job, reference, 8x8 cell); level 0 includes the
+// quarter-pel refinement. Units: nrefs * fcols[level] * frows[level] per job.
+void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, cudaStream_t st);
+
+// Intra SATDs of every candidate block and mode. Units: sb_cols * sb_rows per job.
+void launch_intra(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
+
+// Each reference's best candidate MV per candidate block. Units: nrefs * sb_cols * sb_rows per job.
+void launch_inter(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
+
+// Per-block choice, compound, partition choice and the decision records. Units: superblocks.
+void launch_finalize(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
+
+// Set-up of the constant tables (once per device).
+cudaError_t init_tables();
+
+}  // namespace celv2cu

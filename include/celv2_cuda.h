@@ -1,0 +1,124 @@
+/* celv2_cuda.h: the C ABI of the B200 decision engine (libcelv2_cuda.so).
+ *
+ * The engine is a drop-in third implementation of the reference encoder's DecisionEngine
+ * (src/gpu/decision_engine.h:9-51) next to its CpuEngine and VulkanEngine: it decides every
+ * 64x64 superblock of a frame -- hierarchical motion search over up to 7 references with
+ * quarter-pel refinement, intra / inter / compound SATD scoring and the bottom-up partition
+ * choice -- and emits the decision records of include/celv2_decision.h, byte-identical to the
+ * reference CpuEngine's decisions on the same 8-bit luma planes and lambda. Plain pointers and
+ * sizes only; a C++ adapter deriving from DecisionEngine sits on top.
+ *
+ * Every function returns 0 on success and a negative CELV2_E* code on failure, with a message
+ * for the calling thread in celv2_last_error(). One thread drives launch / prepare of an engine;
+ * the row waits may come from another thread. Several engines may share a GPU.
+ */
+#ifndef CELV2_CUDA_H
+#define CELV2_CUDA_H
+
+#include <stdint.h>
+
+#include "celv2_decision.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CELV2_OK = 0,
+  CELV2_EINVAL = -1,   /* bad argument (the reference throws std::runtime_error / invalid_argument) */
+  CELV2_ECUDA = -2,    /* CUDA runtime error (no device, out of memory, launch failure) */
+  CELV2_ESTATE = -3,   /* call out of order (e.g. a row wait with no launch) */
+};
+
+typedef struct celv2_engine celv2_engine;
+
+/* A frame's luma, as the reference's Frame420 holds it (src/io/y4m.h:11-23): visible width x
+ * height, planes padded by edge replication to pw = (width + 7) & ~7 by ph = (height + 7) & ~7.
+ * Give either the 8-bit plane `y` (Frame420::y, already rounded), or the high-depth plane `hy`
+ * (Frame420::hy) with its bit_depth, which the engine rounds to 8 bits on the device exactly as
+ * round_to_8bit does (src/io/y4m.cpp:28-34). pitch: samples per row (0: pw). */
+typedef struct celv2_frame {
+  int32_t width, height;
+  int32_t pitch;
+  const uint8_t* y;
+  const uint16_t* hy;
+  int32_t bit_depth;
+} celv2_frame;
+
+/* VulkanEngine(width, height, sb_size, device) (src/vk/vk_engine.h:18, vk_engine.cpp:172-180):
+ * throws on a zero size and on sb_size != 64; here CELV2_EINVAL. */
+int celv2_create(int width, int height, int sb_size, int device, celv2_engine** out);
+void celv2_destroy(celv2_engine* e);
+
+/* DecisionEngine::launch (decision_engine.h:12-18; vk_engine.cpp:207-312): queues the decision of
+ * every superblock row and returns. refs nearest first, at most 7; nrefs 0 is a KEY frame.
+ * ref_keys (NULL, or one per reference): a reference whose key was seen before is the same
+ * picture, and its upload, pyramid and phases are reused. src_key: the key a prepare() used.
+ * The inputs are copied before this returns. lambda_q8: the encoder's lambda_q8(qindex)
+ * (src/core/quant.cpp:31-39). Errors as the reference's: a size mismatch or more than 7
+ * references (std::runtime_error there) -> CELV2_EINVAL; a failure leaves no work running. */
+int celv2_launch(celv2_engine* e, const celv2_frame* src, const celv2_frame* refs, int nrefs, int64_t lambda_q8,
+                 const long long* ref_keys, long long src_key);
+
+/* DecisionEngine::prepare (decision_engine.h:19-22; vk_engine.cpp:188-205): starts the next
+ * frame's reference-free work (upload, pyramid, intra SATDs) behind the queued work, on a second
+ * stream. A key < 0 or a size mismatch does nothing. */
+int celv2_prepare(celv2_engine* e, const celv2_frame* next, long long key);
+
+/* DecisionEngine::set_row_streams (decision_engine.h:30-33; vk_engine.cpp:288-294): rows come
+ * back as the first row of each of n runs, then the second, ... (1: top to bottom). */
+int celv2_set_row_streams(celv2_engine* e, int n);
+
+/* Superblock columns and rows of the engine's frames. */
+int celv2_geometry(const celv2_engine* e, int* sb_cols, int* sb_rows);
+
+/* The order the last launch brings rows back in (sb_rows entries). */
+int celv2_row_order(const celv2_engine* e, int* rows);
+
+/* The collect side (DecisionEngine::collect, decision_engine.h:27-29): blocks until superblock
+ * row `row` of the last launch is in host memory and returns its sb_cols records (valid until the
+ * next launch). */
+int celv2_wait_row(celv2_engine* e, int row, const celv2_sb_out** records);
+
+/* Returns with no work of the last launch pending (collect's end). */
+int celv2_finish(celv2_engine* e);
+
+/* The calling thread's last error message ("" if none). */
+const char* celv2_last_error(void);
+
+/* ---- Device-resident path (frames already in HBM; batching) ---- */
+
+/* Uploads a frame into the engine's keyed frame store (pyramid and quarter-pel phases), as a
+ * reference would be; key >= 0. Later launches find it by key. */
+int celv2_upload(celv2_engine* e, const celv2_frame* f, long long key);
+
+/* One batch of frames decided from the frame store: job i decides the frame with key src_keys[i]
+ * against the nrefs[i] frames ref_keys[i][0..]. All jobs' stages run as one launch per stage.
+ * Records stay in device memory unless `to_host` is nonzero, in which case they come back to the
+ * engine's host buffer (celv2_group_records). At most 32 jobs, nsb * jobs within the engine's
+ * group capacity (celv2_create sizes it for 8 frames; celv2_reserve_group raises it). */
+int celv2_launch_group(celv2_engine* e, int njobs, const long long* src_keys, const int* nrefs,
+                       const long long* const* ref_keys, const int64_t* lambda_q8, int to_host);
+int celv2_reserve_group(celv2_engine* e, int frames);
+int celv2_group_records(celv2_engine* e, int job, const celv2_sb_out** records);
+
+/* Drops every frame of the store. */
+int celv2_clear_store(celv2_engine* e);
+
+/* ---- Inspection (tests) ---- */
+
+/* The last launch's motion field of reference r at pyramid level l: cols x rows packed MVs
+ * (mvy << 16 | (mvx & 0xffff)); cols / rows receive the size. Synchronises. */
+int celv2_debug_field(celv2_engine* e, int r, int level, int32_t* out, int* cols, int* rows);
+/* The last launch's intra SATDs: sb_cols * sb_rows * 425 * 13 int32. Synchronises. */
+int celv2_debug_intra(celv2_engine* e, int32_t* out);
+/* The last launch's per-reference bests: sb_cols * sb_rows * 7 * 425 (SATD, packed MV) pairs. */
+int celv2_debug_inter(celv2_engine* e, int32_t* out);
+/* Kernel launches the engine has issued so far (all stages). */
+long long celv2_kernel_launches(const celv2_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CELV2_CUDA_H */

@@ -7,31 +7,13 @@ import subprocess
 
 import numpy as np
 
+from celv2_b200.records import SB_OUT_BYTES, SB_OUT_DTYPE, first_difference, records_equal  # noqa: F401
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libcelv2ref.so")
 
-SB_OUT_BYTES = 38872
 LEVELS = 5
-
-# The record layout of include/celv2_decision.h as a numpy dtype (byte offsets fixed by the C struct).
-SB_OUT_DTYPE = np.dtype(
-    [
-        ("ntree", "<i4"), ("nblocks", "<i4"),
-        ("tree", "u1", 256), ("w4", "u1", 256), ("h4", "u1", 256), ("mode", "u1", 256),
-        ("mvx", "<i2", 256), ("mvy", "<i2", 256),
-        ("ref", "u1", 256), ("ref2", "u1", 256),
-        ("mv2x", "<i2", 256), ("mv2y", "<i2", 256),
-        ("c_inter_cost", "<i8", 425), ("c_intra_cost", "<i8", 425),
-        ("c_mvx", "<i2", 425), ("c_mvy", "<i2", 425), ("c_mv2x", "<i2", 425), ("c_mv2y", "<i2", 425),
-        ("c_ref", "u1", 425), ("c_ref2", "u1", 425), ("c_intra", "u1", 425),
-        ("_pad", "u1", 1),
-        ("c_rcost", "<u4", (7, 425)),
-        ("c_rmvx", "<i2", (7, 425)), ("c_rmvy", "<i2", (7, 425)),
-        ("_tail", "u1", 4),
-    ]
-)
-assert SB_OUT_DTYPE.itemsize == SB_OUT_BYTES
 
 
 def build(reference: bool = True) -> None:
@@ -72,26 +54,6 @@ def _plist(planes):
     for i, p in enumerate(planes):
         arr[i] = _u8p(p)
     return arr
-
-
-def records_equal(a: np.ndarray, b: np.ndarray) -> bool:
-    return a.shape == b.shape and a.tobytes() == b.tobytes()
-
-
-def first_difference(a: np.ndarray, b: np.ndarray):
-    """(superblock, field, index) of the first difference of two record arrays, or None."""
-    if a.shape != b.shape:
-        return ("shape", a.shape, b.shape)
-    for i in range(a.shape[0]):
-        if a[i].tobytes() == b[i].tobytes():
-            continue
-        for name in SB_OUT_DTYPE.names:
-            x, y = np.asarray(a[i][name]), np.asarray(b[i][name])
-            if not np.array_equal(x, y):
-                idx = np.argwhere(x != y)[0]
-                return (i, name, tuple(int(v) for v in idx), x[tuple(idx)].item(), y[tuple(idx)].item())
-        return (i, "padding", None)
-    return None
 
 
 class Oracle:
