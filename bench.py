@@ -1,0 +1,447 @@
+#!/usr/bin/env python
+"""Decision-engine throughput on the 1080p 10-bit mini-GOP workload.
+
+Workload: 1920x1080 4:2:0 10-bit, 17 seeded synthetic frames (8 sinusoids, 12 moving rectangles,
+per-region affine motion up to +-24 px, noise sigma 4), coded as one 16-frame mini-GOP with a hidden
+anchor and a pyramid, --refs 7, qindex 130. Coding order and references follow the reference
+encoder (src/chunk_coder.cpp:213-225,340-430): the KEY frame, the anchor, the pyramid mids (each a
+reference for what follows), then the ten non-reference leaves, which depend on none of each other
+and are decided as one batch. Each frame's references are the reference frames coded before it,
+nearest display distance first, at most 7; source frames stand in for reconstructions (as the
+reference's tools/engine_bench.cpp does). A step decides all 17 frames.
+
+Lines (one JSON line on rank 0):
+  value  -- frames/s with the frames resident in HBM (uploaded before timing), CUDA events on the
+            engine's stream, max over ranks; the leaves run as one batched launch per stage.
+  e2e    -- frames/s through the reference-facing API (launch / prepare / collect per frame, host
+            10-bit planes in, decision records back to host memory), wall clock.
+  roofline, cpu_baseline, clocks, gpu_launches as the harness asks.
+--impl reference times the reference's own CpuEngine (compiled from its sources into oracle/_ref)
+on the host cores, one 7-reference frame of the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1080p10 decision-engine frames/s: plain vs learned-pruned at ≤1% BD-rate loss"
+UNIT = "frames/s"
+W, H, NFRAMES, REFS, QINDEX, SEED = 1920, 1080, 17, 7, 130, 1
+
+
+def mids_of(m: int, refs: int):
+    """The pyramid mids of an m-frame mini-GOP (src/chunk_coder.cpp:213-225): positions, coded order."""
+    mids = []
+
+    def split(lo, hi, level):
+        if hi - lo - 1 < 3 or refs < 3 or len(mids) + 2 >= refs:
+            return
+        mid = (lo + hi) // 2
+        mids.append(mid)
+        split(lo, mid, level + 1)
+        split(mid, hi, level + 1)
+
+    split(-1, m - 1, 1)
+    return mids
+
+
+def mini_gop_plan(nframes: int = NFRAMES, refs: int = REFS):
+    """[(group of (src, [refs nearest first]))] in coding order: KEY, anchor, mids, then the leaves
+    as one group. Frame numbers are display order; frame 0 is the KEY frame."""
+    m = nframes - 1
+    mids = [1 + p for p in mids_of(m, refs)]
+    anchor = m
+    leaves = [d for d in range(1, m) if d not in mids]
+    coded_refs = [0]
+    groups = [[(0, [])]]
+
+    def refs_of(d):
+        order = sorted(coded_refs, key=lambda r: (abs(r - d), r))
+        return order[:refs]
+
+    for d in [anchor] + mids:
+        groups.append([(d, refs_of(d))])
+        coded_refs.append(d)
+    groups.append([(d, refs_of(d)) for d in leaves])
+    return groups
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device, self.rows, self.proc = device, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(rows[0][2]),
+                "samples": len(rows), "reasons": sorted(reasons)}
+
+
+def make_clip(seed: int):
+    from celv2_b200 import synth
+
+    return synth.hd_clip(seed=seed, frames=NFRAMES, width=W, height=H)
+
+
+def dist_setup(gpus: int):
+    """(rank, world, local_rank, dist module or None)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        return rank, world, local, dist
+    return rank, world, local, None
+
+
+def max_over_ranks(v: float, dist, local: int) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist, local):
+    if dist is not None:
+        import torch
+
+        dist.barrier(device_ids=[local])
+        torch.cuda.synchronize(local)
+
+
+# ---------------------------------------------------------------- the reference's CPU engine
+def cpu_reference_sample(clip, threads: int, frames: int = 1):
+    """The reference CpuEngine (oracle/_ref) on `frames` 7-reference leaves; (frames/s, kind, cores, what)."""
+    from celv2_b200 import lam
+    from oracle import Oracle, Reference, reference_available
+
+    plan = mini_gop_plan()
+    leaves = plan[-1][:frames]
+    if reference_available():
+        ref = Reference(lam.table())
+        eng = ref.engine(W, H, threads)
+        eng.hold_frames([f.y for f in clip])
+        t0 = time.perf_counter()
+        for src, refs in leaves:
+            eng.decide_held(src, refs, QINDEX)
+        dt = time.perf_counter() - t0
+        eng.close()
+        kind = "reference"
+    else:
+        o = Oracle()
+        t0 = time.perf_counter()
+        for src, refs in leaves:
+            o.decide(W, H, clip[src].y, [clip[r].y for r in refs], lam.lambda_q8(QINDEX), threads)
+        dt = time.perf_counter() - t0
+        kind = "port"
+    what = (f"{len(leaves)} leaf frame(s) of the 1080p mini-GOP, 7 references each, qindex {QINDEX}, "
+            f"8-bit planes held in the CPU engine, {threads} threads")
+    return len(leaves) / dt, kind, threads, what
+
+
+def run_reference_arm(args):
+    rank, world, local, dist = dist_setup(args.gpus)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    clip = make_clip(SEED)
+    threads = os.cpu_count() or 1
+    from celv2_b200 import lam
+    from oracle import Reference, reference_available
+
+    if not reference_available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "the reference CpuEngine was not compiled (its sources were absent when "
+                                         "oracle/_ref was built)"}))
+        return
+    ref = Reference(lam.table())
+    eng = ref.engine(W, H, threads)
+    eng.hold_frames([f.y for f in clip])
+    leaves = mini_gop_plan()[-1]
+    steps = min(args.steps, 12)
+    for i in range(min(args.warmup, 1)):
+        src, refs = leaves[i % len(leaves)]
+        eng.decide_held(src, refs, QINDEX)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        src, refs = leaves[i % len(leaves)]
+        eng.decide_held(src, refs, QINDEX)
+    dt = time.perf_counter() - t0
+    eng.close()
+    fps = steps / dt
+    sample = (f"one 7-reference leaf frame of the 1080p mini-GOP per step ({steps} timed steps"
+              f"{', capped at 12' if args.steps > 12 else ''}, {min(args.warmup, 1)} warm-up), "
+              f"8-bit planes held in the engine, {threads} host threads")
+    line = {"metric": METRIC, "value": fps, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": dt / steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded 1080p 10-bit clip, rounded to the 8-bit planes the engine scores)",
+            "config": {"workload": "1080p10 mini-GOP of 17 frames, refs 7, qindex 130 (one 7-reference frame per "
+                                   "step on the CPU)", "frames": 1, "refs": 7, "qindex": QINDEX},
+            "cpu_baseline": {"value": fps, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- the CUDA engine
+SAD_OPS = 3          # one SAD sample: subtract, absolute value, accumulate
+H4_OPS = 112         # one 4x4 Hadamard SATD: 16 residuals, 64 butterflies, 16 abs, 16 adds
+RECORD_BYTES = 38872
+
+
+def level_dims(level: int):
+    pw, ph = (W + 7) & ~7, (H + 7) & ~7
+    w, h = pw, ph
+    for _ in range(level):
+        w, h = w // 2, h // 2
+    return w, h, (w + 7) // 8, (h + 7) // 8
+
+
+def plan_counts(plan):
+    """Per step: ME cells per level (summed over references), inter (frame, reference) pairs, frames."""
+    inter_refs = sum(len(refs) for g in plan for _, refs in g)
+    cells = [inter_refs * level_dims(l)[2] * level_dims(l)[3] for l in range(5)]
+    return cells, inter_refs, sum(len(g) for g in plan)
+
+
+def stage_ops(counters, plan, steps):
+    """Integer ops the kernels executed per stage over `steps` steps, from the work counters
+    (searched centres per level, distinct inter MVs, compound tiles) and the fixed per-unit work."""
+    cells, _, frames = plan_counts(plan)
+    nsb = ((W + 63) // 64) * ((H + 63) // 64)
+    ops = {}
+    for l in range(5):
+        centre = (cells[l] * steps * 6 * 64 * SAD_OPS) if l < 4 else 0
+        search = counters[l] * 289 * 64 * SAD_OPS
+        refine = cells[0] * steps * 18 * 4 * H4_OPS if l == 0 else 0
+        ops[f"me_l{l}"] = float(centre + search + refine)
+    ops["intra"] = float(frames * steps * nsb * 2304 * 13 * H4_OPS)
+    ops["inter"] = float(counters[5] * 256 * H4_OPS)
+    ops["finalize"] = float(counters[6] * H4_OPS)
+    return ops
+
+
+def stage_bytes(plan, steps):
+    """Minimum HBM bytes per stage over `steps` steps: every input read once, every output written once."""
+    cells, inter_refs, frames = plan_counts(plan)
+    nsb = ((W + 63) // 64) * ((H + 63) // 64)
+    out = {}
+    for l in range(5):
+        w, h, c, r = level_dims(l)
+        out[f"me_l{l}"] = float(steps * inter_refs * (2 * w * h + 3 * 4 * c * r))
+    w0, h0 = level_dims(0)[:2]
+    out["intra"] = float(steps * frames * (w0 * h0 + nsb * 425 * 13 * 4))
+    out["inter"] = float(steps * inter_refs * (2 * w0 * h0 + nsb * 425 * 8))
+    out["finalize"] = float(steps * (inter_refs * nsb * 425 * 8 + frames * nsb * (425 * 13 * 4 + RECORD_BYTES)))
+    return out
+
+
+def run_cuda_arm(args):
+    import torch
+
+    from celv2_b200 import engine as E
+    from celv2_b200 import lam
+    from celv2_b200.records import DecisionMap
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    clip = make_clip(SEED + rank)
+    plan = mini_gop_plan()
+    eng = E.CudaEngine(W, H, device=local)
+    eng.reserve_group(max(len(g) for g in plan))
+    for i, f in enumerate(clip):
+        eng.upload(f.hy, i)  # 10-bit planes; the device rounds them to the 8-bit samples it scores
+    stream = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{local}")
+
+    def step():
+        for group in plan:
+            eng.launch_group([s for s, _ in group], [r for _, r in group], QINDEX)
+
+    for _ in range(args.warmup):
+        step()
+    eng.finish()
+    barrier(dist, local)
+    launches0 = eng.kernel_launches()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize(local)
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        end.record(stream)
+        end.synchronize()
+    launches = eng.kernel_launches() - launches0
+    ms = start.elapsed_time(end)
+    ms_max = max_over_ranks(ms, dist, local)
+    frames = NFRAMES * args.steps * world
+    value = frames / (ms_max / 1e3)
+
+    # stage times (a separate pass with an event pair around every stage launch)
+    eng.stage_timing(True)
+    eng.stage_times()
+    eng.work_counters()
+    for _ in range(2):
+        step()
+    st = eng.stage_times()
+    counters = eng.work_counters()
+    eng.stage_timing(False)
+    dominant = max(st, key=lambda k: st[k][0])
+    dom_ms, dom_n = st[dominant]
+
+    # e2e through the reference-facing API: host 10-bit planes in, records to host memory
+    e2e_steps = max(1, min(args.steps, 3))
+    h2d = d2h = 0
+    barrier(dist, local)
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        order = [(src, refs) for group in plan for src, refs in group]
+        key = lambda d: (s + 1) * 1000 + d  # noqa: E731 -- new pictures every step (reconstructions differ)
+        for i, (src, refs) in enumerate(order):
+            dm = DecisionMap()
+            eng.launch(clip[src].hy, [clip[r].hy for r in refs], QINDEX, dm, [key(r) for r in refs], key(src))
+            if i + 1 < len(order):
+                eng.prepare(clip[order[i + 1][0]].hy, key(order[i + 1][0]))
+            eng.collect(dm, E.RowGate())
+    t_e2e = time.perf_counter() - t0
+    t_e2e = max_over_ranks(t_e2e, dist, local)
+    plane = clip[0].hy.nbytes
+    ref_frames = {r for group in plan for _, refs in group for r in refs}
+    h2d = (NFRAMES + len(ref_frames)) * plane
+    d2h = NFRAMES * eng.sb_cols * eng.sb_rows * 38872
+    e2e = NFRAMES * e2e_steps * world / t_e2e
+
+    line = None
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        int_peak = E.int_peak(local) / 1e9
+        ops = stage_ops(counters, plan, 2)
+        achieved = ops.get(dominant, 0.0) / dom_n / (dom_ms / dom_n / 1e3) / 1e9 if dom_n else 0.0
+        traffic = None
+        tr_path = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tr_path):
+            traffic = json.load(open(tr_path)).get(dominant)
+        hbm_bytes = stage_bytes(plan, 2).get(dominant, 0.0)
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        roofline = {"bound": "int32", "kernel": dominant, "achieved": achieved, "peak": int_peak, "unit": "Gop/s",
+                    "frac": achieved / int_peak if int_peak else None, "traffic": traffic,
+                    "peak_source": "measured in this run: INT32 add/xor chains on every SM (celv2_int_peak)",
+                    "launch_ms": dom_ms / max(1, dom_n),
+                    "hbm": {"achieved": hbm_bytes / dom_n / (dom_ms / dom_n / 1e3) / 1e9 if dom_n else 0.0,
+                            "peak": hbm_peak, "unit": "GB/s",
+                            "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"},
+                    "stages_ms_per_step": {k: v[0] / 2 for k, v in st.items()},
+                    "stages_int_frac": {k: (ops[k] / (st[k][0] / 1e3) / 1e9 / int_peak if st[k][0] else None)
+                                        for k in ops}}
+        roofline["hbm"]["frac"] = roofline["hbm"]["achieved"] / hbm_peak
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            fps, kind, cores, what = cpu_reference_sample(clip, os.cpu_count() or 1)
+            cpu = {"value": fps, "unit": UNIT, "cores": cores, "kind": kind, "sample": what}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic (seeded 1080p 10-bit clips, one per rank; the engine scores their 8-bit rounding)",
+                "variant": "plain (exhaustive CUDA engine)",
+                "config": {"workload": "1080p10 mini-GOP: 17 frames 1920x1080, hidden anchor + pyramid, refs 7, "
+                                       "qindex 130; leaves batched", "frames_per_step": NFRAMES, "refs": REFS,
+                           "qindex": QINDEX, "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (17 resident frames with phase planes, ~1.2 GB per rank)"},
+                "clocks": clocks.summary(), "gpu_launches": launches,
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": e2e_steps, "api": "launch/prepare/collect per frame (celv2_launch, celv2_wait_row)"},
+                "roofline": roofline, "cpu_baseline": cpu}
+        print(json.dumps(line))
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "cuda":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_cuda_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -30,6 +30,7 @@
 #include "tables.h"
 
 namespace celv2cu {
+cudaError_t measure_int_peak(int device, double* ops_per_s);
 cudaError_t inter_attributes();
 cudaError_t intra_attributes();
 cudaError_t finalize_attributes();
@@ -138,6 +139,9 @@ struct Stage {
   bool pending = false;
 };
 
+// Stages timed by CUDA events when stage timing is on (celv2_stage_timing).
+enum StageId { kStUpload, kStPhases, kStMe4, kStMe3, kStMe2, kStMe1, kStMe0, kStIntra, kStInter, kStFinalize, kStages };
+
 // Per-frame device buffers of a decision.
 struct JobBuffers {
   int* fields = nullptr;     // kMaxRefs * field_ints
@@ -182,6 +186,50 @@ struct celv2_engine {
   celv2_sb_out* group_host = nullptr;
   int group_jobs = 0;
   long long kernel_launches = 0;
+  // stage timing: an event pair around each stage launch, harvested when the stream is idle
+  bool timing = false;
+  struct Timed {
+    int stage;
+    cudaEvent_t a, b;
+  };
+  std::vector<Timed> timed;
+  std::vector<cudaEvent_t> event_pool;
+  double stage_ms[kStages] = {};
+  long long stage_n[kStages] = {};
+  unsigned long long* stats = nullptr;  // device work counters (kStats), while timing
+
+  template <typename F>
+  void stage(int id, cudaStream_t stream, F&& f) {
+    if (!timing) {
+      f();
+      return;
+    }
+    cudaEvent_t ev[2];
+    for (cudaEvent_t& e : ev) {
+      if (event_pool.empty()) {
+        CK(cudaEventCreate(&e));
+      } else {
+        e = event_pool.back();
+        event_pool.pop_back();
+      }
+    }
+    CK(cudaEventRecord(ev[0], stream));
+    f();
+    CK(cudaEventRecord(ev[1], stream));
+    timed.push_back({id, ev[0], ev[1]});
+  }
+
+  void harvest() {
+    for (const Timed& t : timed) {
+      CK(cudaEventSynchronize(t.b));
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, t.a, t.b));
+      stage_ms[t.stage] += ms;
+      stage_n[t.stage]++;
+      event_pool.push_back(t.a), event_pool.push_back(t.b);
+    }
+    timed.clear();
+  }
 
   ~celv2_engine() {
     cudaSetDevice(device);
@@ -199,6 +247,9 @@ struct celv2_engine {
     cudaFreeHost(host_out);
     cudaFreeHost(group_host);
     for (cudaEvent_t e : row_done) cudaEventDestroy(e);
+    for (const Timed& t : timed) cudaEventDestroy(t.a), cudaEventDestroy(t.b);
+    cudaFree(stats);
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     cudaFree(djobs);
     cudaFreeHost(ring);
     for (cudaEvent_t e : ring_done)
@@ -301,13 +352,15 @@ struct celv2_engine {
       for (int r = 0; r < g.ph; r++) std::memcpy((uint8_t*)sg.host + r * row, src + r * spitch, row);
     }
     CK(cudaMemcpyAsync(sg.dev, sg.host, row * g.ph, cudaMemcpyHostToDevice, stream));
-    if (wide)
-      launch_expand_u16((const uint16_t*)sg.dev, g.pw, f->bit_depth, s.pyr.lv[0], stream);
-    else
-      launch_expand_u8((const uint8_t*)sg.dev, g.pw, s.pyr.lv[0], stream);
+    stage(kStUpload, stream, [&] {
+      if (wide)
+        launch_expand_u16((const uint16_t*)sg.dev, g.pw, f->bit_depth, s.pyr.lv[0], stream);
+      else
+        launch_expand_u8((const uint8_t*)sg.dev, g.pw, s.pyr.lv[0], stream);
+    });
     CK(cudaEventRecord(sg.done, stream));
     sg.pending = true;
-    launch_pyramid(s.pyr, stream);
+    stage(kStUpload, stream, [&] { launch_pyramid(s.pyr, stream); });
     kernel_launches += 1 + (kLevels - 1);
     s.phases = false;
     if (phases) make_phases(s, stream);
@@ -315,7 +368,7 @@ struct celv2_engine {
 
   void make_phases(Slot& s, cudaStream_t stream) {
     if (s.phases) return;
-    launch_phases(s.pyr.lv[0], stream);
+    stage(kStPhases, stream, [&] { launch_phases(s.pyr.lv[0], stream); });
     kernel_launches++;
     s.phases = true;
   }
@@ -364,6 +417,7 @@ struct celv2_engine {
     job.out = b.out;
     job.lam = lam;
     job.items = items;
+    job.stats = timing ? stats : nullptr;
   }
 
   // Queues the copy of n descriptors to dst (device) through the pinned ring.
@@ -386,7 +440,10 @@ struct celv2_engine {
     w.njobs = n;
     for (int l = kLevels - 1; l >= 0; l--) {
       for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].nrefs * jobs[j].fcols[l] * jobs[j].frows[l];
-      if (w.prefix[n] > 0) launch_me_level(djobs, w, l, stream), kernel_launches++;
+      if (w.prefix[n] > 0) {
+        stage(kStMe0 - l, stream, [&] { launch_me_level(djobs, w, l, stream); });
+        kernel_launches++;
+      }
     }
     for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + (need_intra[j] ? jobs[j].sb_cols * jobs[j].sb_rows : 0);
     if (w.prefix[n] > 0) {
@@ -395,21 +452,24 @@ struct celv2_engine {
       for (int j = 0; j < n; j++)
         if (need_intra[j]) sub.push_back(jobs[j]);
       if ((int)sub.size() == n) {
-        launch_intra(djobs, w, stream);
+        stage(kStIntra, stream, [&] { launch_intra(djobs, w, stream); });
       } else {
         // the flagged jobs' descriptors go after the batch's
         put_jobs(sub.data(), (int)sub.size(), djobs + n, stream);
         WorkList ws{};
         ws.njobs = (int)sub.size();
         for (int j = 0; j < ws.njobs; j++) ws.prefix[j + 1] = ws.prefix[j] + sub[j].sb_cols * sub[j].sb_rows;
-        launch_intra(djobs + n, ws, stream);
+        stage(kStIntra, stream, [&] { launch_intra(djobs + n, ws, stream); });
       }
       kernel_launches++;
     }
     for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].nrefs * jobs[j].sb_cols * jobs[j].sb_rows;
-    if (w.prefix[n] > 0) launch_inter(djobs, w, stream), kernel_launches++;
+    if (w.prefix[n] > 0) {
+      stage(kStInter, stream, [&] { launch_inter(djobs, w, stream); });
+      kernel_launches++;
+    }
     for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].sb_cols * jobs[j].sb_rows;
-    launch_finalize(djobs, w, stream);
+    stage(kStFinalize, stream, [&] { launch_finalize(djobs, w, stream); });
     kernel_launches++;
     CK(cudaGetLastError());
   }
@@ -417,6 +477,10 @@ struct celv2_engine {
   void wait_idle() {
     CK(cudaStreamSynchronize(st));
     pending = false;
+    if (!timed.empty()) {
+      CK(cudaStreamSynchronize(prep_st));
+      harvest();
+    }
   }
 
   void launch(const celv2_frame* src, const celv2_frame* refs, int nrefs, long long lam, const long long* keys,
@@ -497,7 +561,7 @@ struct celv2_engine {
     WorkList w{};
     w.njobs = 1;
     w.prefix[1] = g.nsb;
-    launch_intra(dprep, w, prep_st);
+    stage(kStIntra, prep_st, [&] { launch_intra(dprep, w, prep_st); });
     kernel_launches++;
     CK(cudaGetLastError());
     CK(cudaEventRecord(prep_done, prep_st));
@@ -738,5 +802,60 @@ int celv2_debug_inter(celv2_engine* e, int32_t* out) {
 }
 
 long long celv2_kernel_launches(const celv2_engine* e) { return e ? e->kernel_launches : 0; }
+
+int celv2_stream(const celv2_engine* e, void** stream) {
+  return guarded([&] {
+    if (!e || !stream) invalid("null argument");
+    *stream = e->st;
+  });
+}
+
+int celv2_stage_timing(celv2_engine* e, int enable) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    e->timing = enable != 0;
+    if (e->timing && !e->stats) {
+      CK(cudaMalloc(&e->stats, kStats * sizeof(unsigned long long)));
+      CK(cudaMemset(e->stats, 0, kStats * sizeof(unsigned long long)));
+    }
+  });
+}
+
+int celv2_work_counters(celv2_engine* e, unsigned long long* out, int n) {
+  return guarded([&] {
+    if (!e || !out) invalid("null argument");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    CK(cudaStreamSynchronize(e->prep_st));
+    unsigned long long v[kStats] = {};
+    if (e->stats) {
+      CK(cudaMemcpy(v, e->stats, sizeof v, cudaMemcpyDeviceToHost));
+      CK(cudaMemset(e->stats, 0, sizeof v));
+    }
+    for (int i = 0; i < n && i < kStats; i++) out[i] = v[i];
+  });
+}
+
+int celv2_stage_times(celv2_engine* e, double* ms, long long* launches, int n) {
+  return guarded([&] {
+    if (!e || !ms || !launches) invalid("null argument");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    CK(cudaStreamSynchronize(e->prep_st));
+    e->harvest();
+    for (int i = 0; i < n && i < kStages; i++) ms[i] = e->stage_ms[i], launches[i] = e->stage_n[i];
+    std::fill(e->stage_ms, e->stage_ms + kStages, 0.0);
+    std::fill(e->stage_n, e->stage_n + kStages, 0LL);
+  });
+}
+
+int celv2_int_peak(int device, double* ops_per_s) {
+  return guarded([&] {
+    if (!ops_per_s) invalid("null argument");
+    CK(measure_int_peak(device, ops_per_s));
+  });
+}
 
 }  // extern "C"

@@ -76,6 +76,11 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(const FrameJob* __rest
     S.inter_mv[b] = a >= 0 ? rmv[a] : 0;
     S.inter_ref[b] = a >= 0 ? a : 0;
     const bool comp = second >= 0 && compound_pair_ok(a, second, nrefs);
+    if (comp && job.stats) {
+      int bx, by, bw, bh;
+      sb_block_geom(b, bx, by, bw, bh);
+      atomicAdd(job.stats + kStatCompoundTiles, (unsigned long long)(bw / 4) * (bh / 4));
+    }
     S.comp_a[b] = comp ? a : -1;
     S.comp_b[b] = comp ? second : 0;
     S.comp_mv0[b] = comp ? rmv[a] : 0;

@@ -154,6 +154,7 @@ __global__ void __launch_bounds__(kInterThreads) k_inter(const FrameJob* __restr
   __syncthreads();
   if (tid < kNb) S.dmap[tid] = (unsigned char)S.first_idx[firstj];
   const int nd = S.nd;
+  if (tid == 0 && job.stats) atomicAdd(job.stats + kStatInterMvs, (unsigned long long)nd);
 
   // 2. per 8x8 cell and distinct MV: the tile SATD halves
   {

@@ -170,7 +170,10 @@ __global__ void __launch_bounds__(kMeWarps * 32) k_me_level(const FrameJob* __re
     }
     mx = cxq, my = cyq;
   }
-  if (lane == 0) job.field[r][level][cell] = pack_mv(mx, my);
+  if (lane == 0) {
+    job.field[r][level][cell] = pack_mv(mx, my);
+    if (job.stats) atomicAdd(job.stats + level, two ? 2ull : 1ull);
+  }
 }
 
 void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, cudaStream_t st) {

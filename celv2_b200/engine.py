@@ -59,7 +59,15 @@ SIGNATURES = {
     "celv2_debug_intra": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "celv2_debug_inter": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "celv2_kernel_launches": (C.c_longlong, [C.c_void_p]),
+    "celv2_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "celv2_stage_timing": (C.c_int, [C.c_void_p, C.c_int]),
+    "celv2_stage_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_int]),
+    "celv2_int_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "celv2_work_counters": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int]),
 }
+
+STAGE_NAMES = ["upload+pyramid", "phases", "me_l4", "me_l3", "me_l2", "me_l1", "me_l0", "intra", "inter",
+               "finalize"]
 
 
 def library():
@@ -287,6 +295,27 @@ class CudaEngine:
     def kernel_launches(self) -> int:
         return int(library().celv2_kernel_launches(self._h))
 
+    def stream(self) -> int:
+        p = C.c_void_p()
+        _check(library().celv2_stream(self._h, C.byref(p)))
+        return p.value or 0
+
+    def stage_timing(self, enable: bool) -> None:
+        _check(library().celv2_stage_timing(self._h, 1 if enable else 0))
+
+    def work_counters(self) -> list[int]:
+        """[searched centres at levels 0..4, distinct inter MVs, compound tiles, 0] since the last call."""
+        arr = (C.c_ulonglong * 8)()
+        _check(library().celv2_work_counters(self._h, arr, 8))
+        return list(arr)
+
+    def stage_times(self) -> dict:
+        """{stage: (milliseconds, launches)} since the last call (stage timing must be on)."""
+        n = len(STAGE_NAMES)
+        ms, cnt = (C.c_double * n)(), (C.c_longlong * n)()
+        _check(library().celv2_stage_times(self._h, ms, cnt, n))
+        return {STAGE_NAMES[i]: (ms[i], cnt[i]) for i in range(n)}
+
     # ---- inspection ----
     def debug_field(self, r: int, level: int) -> np.ndarray:
         pw, ph = (self.width + 7) & ~7, (self.height + 7) & ~7
@@ -309,6 +338,13 @@ class CudaEngine:
         out = np.zeros((self.sb_cols * self.sb_rows, 7, 425, 2), np.int32)
         _check(library().celv2_debug_inter(self._h, out.ctypes.data_as(C.POINTER(C.c_int32))))
         return out
+
+
+def int_peak(device: int = 0) -> float:
+    """Measured INT32 ops/s of the GPU (the roofline denominator of the integer kernels)."""
+    v = C.c_double()
+    _check(library().celv2_int_peak(device, C.byref(v)))
+    return v.value
 
 
 def unpack_field(packed: np.ndarray):

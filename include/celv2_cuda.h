@@ -117,6 +117,26 @@ int celv2_debug_inter(celv2_engine* e, int32_t* out);
 /* Kernel launches the engine has issued so far (all stages). */
 long long celv2_kernel_launches(const celv2_engine* e);
 
+/* ---- Measurement ---- */
+
+/* The engine's main stream (a cudaStream_t), for timing events around its work. */
+int celv2_stream(const celv2_engine* e, void** stream);
+/* Stage timing: when enabled, every stage launch is bracketed by CUDA events on its stream.
+ * celv2_stage_times returns (and resets) the summed milliseconds and launch counts per stage, in
+ * the order: uploads (8-bit level 0 + pyramid), quarter-pel phases, motion search levels 4, 3, 2,
+ * 1, 0, intra, inter, finalize (CELV2_STAGES entries). */
+#define CELV2_STAGES 10
+int celv2_stage_timing(celv2_engine* e, int enable);
+int celv2_stage_times(celv2_engine* e, double* ms, long long* launches, int n);
+/* Work the kernels executed while stage timing was on, then reset: [l] motion-search centres
+ * searched at level l (0..4), [5] distinct candidate MVs summed over (superblock, reference),
+ * [6] compound 4x4 tiles (CELV2_WORK_COUNTERS entries). */
+#define CELV2_WORK_COUNTERS 8
+int celv2_work_counters(celv2_engine* e, unsigned long long* out, int n);
+/* The GPU's measured INT32 throughput (integer ops per second): the roofline denominator of the
+ * integer-bound decision kernels. */
+int celv2_int_peak(int device, double* ops_per_s);
+
 #ifdef __cplusplus
 }
 #endif
