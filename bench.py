@@ -250,8 +250,12 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------- the CUDA engine
-SAD_OPS = 3          # one SAD sample: subtract, absolute value, accumulate
-H4_OPS = 112         # one 4x4 Hadamard SATD: 16 residuals, 64 butterflies, 16 abs, 16 adds
+# Integer ops counted as the 32-bit instructions the arithmetic needs, so they compare with the
+# measured INT32 instruction rate: a 4-sample SAD word is one byte-SIMD absolute difference plus
+# one accumulate (2 ops, i.e. 0.5 per sample); a 4x4 Hadamard SATD is 16 residual subtracts,
+# 64 butterflies, 16 absolute values and 16 adds (112 ops).
+SAD_OPS = 0.5
+H4_OPS = 112
 RECORD_BYTES = 38872
 
 
@@ -427,6 +431,23 @@ def run_cuda_arm(args):
     return line
 
 
+def run_profile_case(args):
+    """The small case for ncu: one 7-reference 1080p leaf decided twice, frames resident in HBM
+    (8 frames with phase planes, about 0.6 GB). Kernel order per decision: k_me_level x5
+    (levels 4..0), k_intra, k_inter, k_finalize."""
+    from celv2_b200 import engine as E
+
+    clip = make_clip(SEED)[:8]
+    eng = E.CudaEngine(W, H)
+    for i, f in enumerate(clip):
+        eng.upload(f.hy, i)
+    for _ in range(2):
+        eng.launch_group([7], [[6, 5, 4, 3, 2, 1, 0]], QINDEX)
+    eng.finish()
+    eng.close()
+    print("profile case: done")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -434,7 +455,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", action="store_true", help="the small case for ncu captures")
     args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args)
+        return
     if args.warmup < 3 and args.impl == "cuda":
         args.warmup = 3
     if args.impl == "reference":

@@ -55,7 +55,6 @@ struct FrameJob {
   int2* inter;             // [sb][kMaxRefs][kBlocks]: (best SATD, packed MV)
   celv2_sb_out* out;       // [sb]
   long long lam;           // lambda_q8
-  const uint32_t* items;   // the superblock's (block, tile) work items (tables.h)
   // Work counters for the roofline (null unless stage timing is on): [l] searched centres at
   // level l, [5] distinct MVs summed over (superblock, reference), [6] compound 4x4 tiles.
   unsigned long long* stats;

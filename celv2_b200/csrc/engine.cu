@@ -31,6 +31,7 @@
 
 namespace celv2cu {
 cudaError_t measure_int_peak(int device, double* ops_per_s);
+cudaError_t me_attributes();
 cudaError_t inter_attributes();
 cudaError_t intra_attributes();
 cudaError_t finalize_attributes();
@@ -69,19 +70,17 @@ int guarded(F&& f) {
 }
 
 std::mutex g_init_mu;
-std::vector<uint32_t*> g_items;  // per device: the (block, tile) item table, made once
+std::vector<char> g_ready;  // per device: kernel attributes set
 
-const uint32_t* init_device(int dev) {
+void init_device(int dev) {
   std::lock_guard<std::mutex> lk(g_init_mu);
-  if ((int)g_items.size() <= dev) g_items.resize(dev + 1, nullptr);
-  if (g_items[dev]) return g_items[dev];
+  if ((int)g_ready.size() <= dev) g_ready.resize(dev + 1, 0);
+  if (g_ready[dev]) return;
+  CK(me_attributes());
   CK(inter_attributes());
   CK(intra_attributes());
   CK(finalize_attributes());
-  uint32_t* items = nullptr;
-  CK(make_items(&items));
-  g_items[dev] = items;
-  return items;
+  g_ready[dev] = 1;
 }
 
 size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
@@ -155,7 +154,6 @@ struct JobBuffers {
 struct celv2_engine {
   int device = 0;
   Geometry g;
-  const uint32_t* items = nullptr;
   cudaStream_t st = nullptr, prep_st = nullptr;
   cudaEvent_t prep_done = nullptr;
   std::vector<Slot*> store;      // keyed frames (references, resident frames)
@@ -274,7 +272,7 @@ struct celv2_engine {
   void init(int width, int height, int dev) {
     device = dev;
     CK(cudaSetDevice(dev));
-    items = init_device(dev);
+    init_device(dev);
     g.set(width, height);
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&prep_st, cudaStreamNonBlocking));
@@ -416,7 +414,6 @@ struct celv2_engine {
     job.inter = b.inter;
     job.out = b.out;
     job.lam = lam;
-    job.items = items;
     job.stats = timing ? stats : nullptr;
   }
 
@@ -439,7 +436,7 @@ struct celv2_engine {
     WorkList w{};
     w.njobs = n;
     for (int l = kLevels - 1; l >= 0; l--) {
-      for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].nrefs * jobs[j].fcols[l] * jobs[j].frows[l];
+      for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + me_units(jobs[j].nrefs, jobs[j].fcols[l], jobs[j].frows[l]);
       if (w.prefix[n] > 0) {
         stage(kStMe0 - l, stream, [&] { launch_me_level(djobs, w, l, stream); });
         kernel_launches++;

@@ -93,13 +93,14 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(const FrameJob* __rest
   if (nrefs >= 2) {
     const DevPlane cur = job.cur.lv[0];
     for (int item = tid; item < kItems; item += kFinThreads) {
-      const uint32_t it = job.items[item];
-      const int b = item_block(it), width = item_width(item);
+      int b, tx, ty;
+      item_decode(item, b, tx, ty);
+      const int width = item_width(item);
       int s = 0;
       if (S.comp_a[b] >= 0) {  // uniform over the block's segment
         const DevPlane r0 = job.ref[S.comp_a[b]].lv[0], r1 = job.ref[S.comp_b[b]].lv[0];
         const int m0 = S.comp_mv0[b], m1 = S.comp_mv1[b];
-        const int x = ox + item_tx(it) * 4, y = oy + item_ty(it) * 4;
+        const int x = ox + tx * 4, y = oy + ty * 4;
         const int mx0 = mv_x(m0), my0 = mv_y(m0), mx1 = mv_x(m1), my1 = mv_y(m1);
         int d[16];
 #pragma unroll

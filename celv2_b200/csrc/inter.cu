@@ -108,7 +108,7 @@ __device__ __forceinline__ int block_satd(const InterSmem& S, int b, int d) {
   }
 }
 
-__global__ void __launch_bounds__(kInterThreads) k_inter(const FrameJob* __restrict__ jobs, WorkList w) {
+__global__ void __launch_bounds__(kInterThreads, 2) k_inter(const FrameJob* __restrict__ jobs, WorkList w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   InterSmem& S = *reinterpret_cast<InterSmem*>(smem_raw);
   const int tid = threadIdx.x;

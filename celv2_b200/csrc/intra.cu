@@ -5,12 +5,14 @@
 // square are never intra (kMaxBlockSize 32, :39), so 420 blocks x 13 modes per superblock.
 //
 // One CTA per superblock:
-//  1. the source samples the predictions and residuals read -- rows and columns -1 .. 95 around
-//     the superblock origin (above-right / below-left edges reach w + h - 1 past a block) -- are
-//     staged in shared memory from the margin plane (which already holds the clamped values);
-//  2. every block's DC value is computed once;
-//  3. the 2304 (block, 4x4 tile) items are spread over the threads; each computes its tile's
-//     13 predictions and Hadamards, and a segmented shuffle reduction sums a block's tiles.
+//  1. the source samples around the superblock -- rows and columns -1 .. 95 from its origin
+//     (above-right and below-left edges reach w + h - 1 past a block) -- are staged in shared
+//     memory from the margin plane, which already holds the clamped values;
+//  2. every block's above and left edge arrays, k = -1 .. w + h - 1, are built once with the
+//     frame-edge rules applied (128 outside the frame, the corner rule at k = -1), and its DC;
+//  3. the 2304 (block, 4x4 tile) items are spread over the threads; each predicts its tile under
+//     the 13 modes from the edge arrays alone (no per-sample rule branches) and takes the
+//     Hadamards; a segmented shuffle reduction sums a block's tiles per mode.
 // The output is raw SATDs; the finalize stage adds lambda * bits (which depend on whether the
 // frame has references, unknown when prepare() runs this ahead of its launch).
 #include "kernels.h"
@@ -21,87 +23,35 @@ namespace celv2cu {
 constexpr int kIntraThreads = 256;
 constexpr int kRegion = 97;   // local rows / columns -1 .. 95
 constexpr int kRegionStride = 100;
+constexpr int kEdges = 7588;  // edge entries of the blocks of levels 1-3 (see edge_offset)
 
 struct IntraSmem {
   uint8_t px[kRegion * kRegionStride];
+  uint8_t above[kEdges], left[kEdges];
   int dc[kBlocks];
   int acc[kBlocks][kModes];
 };
 
-// A block's view of the staged samples: local coordinates relative to the superblock origin.
-struct IntraBlock {
-  const uint8_t* px;
-  int x, y, w, h;     // local block position and size
-  bool top, left;     // the block touches the frame's top / left edge
-  __device__ __forceinline__ int s(int ly, int lx) const { return px[(ly + 1) * kRegionStride + lx + 1]; }
-  // edge_above / edge_left (intra_common.h:47-56)
-  __device__ __forceinline__ int above(int k) const {
-    if (top) return 128;
-    if (k < 0 && left) return s(y - 1, x);
-    return s(y - 1, x + k);
-  }
-  __device__ __forceinline__ int leftc(int k) const {
-    if (left) return 128;
-    if (k < 0 && top) return s(y, x - 1);
-    return s(y + k, x - 1);
-  }
-};
-
-__device__ __forceinline__ int dr_derivative(int a) { return a == 23 ? 151 : a == 45 ? 64 : 27; }
-
-// dr_prediction z1 / z2 / z3 without edge filter (intra_common.h:61-85). Not inlined: the six
-// directional modes share one copy, which keeps the per-tile loop within the register budget.
-__device__ __noinline__ int dir_pred(const IntraBlock& B, int angle, int i, int j) {
-  const int last = B.w + B.h - 1;
-  if (angle < 90) {
-    const int pos = (i + 1) * dr_derivative(angle), base = (pos >> 6) + j, shift = (pos & 63) >> 1;
-    const int a0 = B.above(base < last ? base : last), a1 = B.above(base + 1 < last ? base + 1 : last);
-    return (a0 * (32 - shift) + a1 * shift + 16) >> 5;
-  }
-  if (angle > 180) {
-    const int pos = (j + 1) * dr_derivative(270 - angle), base = (pos >> 6) + i, shift = (pos & 63) >> 1;
-    const int l0 = B.leftc(base < last ? base : last), l1 = B.leftc(base + 1 < last ? base + 1 : last);
-    return (l0 * (32 - shift) + l1 * shift + 16) >> 5;
-  }
-  const int px = (j << 6) - (i + 1) * dr_derivative(180 - angle);
-  const int bx = px >= 0 ? px >> 6 : -((-px + 63) >> 6);
-  if (bx >= -1) {
-    const int shift = (px - bx * 64) >> 1;
-    return (B.above(bx) * (32 - shift) + B.above(bx + 1) * shift + 16) >> 5;
-  }
-  const int py = (i << 6) - (j + 1) * dr_derivative(angle - 90);
-  const int by = py >= 0 ? py >> 6 : -((-py + 63) >> 6);
-  const int shift = (py - by * 64) >> 1;
-  const int b0 = by < -1 ? -1 : by, b1 = by + 1 < -1 ? -1 : by + 1;
-  return (B.leftc(b0) * (32 - shift) + B.leftc(b1) * shift + 16) >> 5;
+// Where block b's edge arrays start (b >= 5): a square of side s holds its whole block
+// (2s + 1 entries) then its four halves (1.5s + 1 each); levels 1, 2, 3 follow each other.
+__device__ __forceinline__ int edge_offset(int b) {
+  const int sq = b / 5, kind = b - sq * 5;
+  const int level = sq >= 21 ? 3 : sq >= 5 ? 2 : 1;
+  const int s = 64 >> level, per_sq = 8 * s + 5;
+  const int base = level == 1 ? 0 : level == 2 ? 4 * 261 : 4 * 261 + 16 * 133;
+  const int idx = sq - sb_level_offset(level);
+  return base + idx * per_sq + (kind == 0 ? 0 : (2 * s + 1) + (kind - 1) * (s + s / 2 + 1));
 }
 
-// intra_pred (intra_common.h:89-118) for modes 1..12 at block sample (i, j).
-__device__ __forceinline__ int intra_pred(const IntraBlock& B, int mode, int i, int j) {
-  switch (mode) {
-    case 1: return B.top ? 128 : B.s(B.y - 1, B.x + j);
-    case 2: return B.left ? 128 : B.s(B.y + i, B.x - 1);
-    case 3: {
-      const int a = B.top ? 128 : B.s(B.y - 1, B.x + j), l = B.left ? 128 : B.s(B.y + i, B.x - 1);
-      const int tr = B.top ? 128 : B.s(B.y - 1, B.x + B.w - 1), bl = B.left ? 128 : B.s(B.y + B.h - 1, B.x - 1);
-      const int den = B.w + B.h + 2, num = (B.h - i) * a + (i + 1) * bl + (B.w - j) * l + (j + 1) * tr;
-      return (num + den / 2) / den;
-    }
-    case 4: return ((B.h - 1 - i) * B.above(j) + (i + 1) * B.leftc(B.h - 1) + B.h / 2) / B.h;
-    case 5: return ((B.w - 1 - j) * B.leftc(i) + (j + 1) * B.above(B.w - 1) + B.w / 2) / B.w;
-    case 6: {
-      const int a = B.above(j), l = B.leftc(i), tl = B.above(-1);
-      const int base = a + l - tl, pa = abs(base - a), pl = abs(base - l), ptl = abs(base - tl);
-      return pl <= pa && pl <= ptl ? l : pa <= ptl ? a : tl;
-    }
-    default: {
-      constexpr int kAngle[6] = {45, 67, 113, 135, 157, 203};
-      return dir_pred(B, kAngle[mode - 7], i, j);
-    }
-  }
+// n / d for 0 <= n < 2^20, from a float estimate corrected to the exact quotient.
+__device__ __forceinline__ int exact_div(int n, int d, float rcp) {
+  int q = __float2int_rz((float)n * rcp);
+  if ((q + 1) * d <= n) q++;
+  if (q * d > n) q--;
+  return q;
 }
 
-__global__ void __launch_bounds__(kIntraThreads) k_intra(const FrameJob* __restrict__ jobs, WorkList w) {
+__global__ void __launch_bounds__(kIntraThreads, 3) k_intra(const FrameJob* __restrict__ jobs, WorkList w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   IntraSmem& S = *reinterpret_cast<IntraSmem*>(smem_raw);
   const int tid = threadIdx.x;
@@ -112,53 +62,167 @@ __global__ void __launch_bounds__(kIntraThreads) k_intra(const FrameJob* __restr
   const int ox = sbx * 64, oy = sby * 64;
   const DevPlane src = job.cur.lv[0];
 
-  // 1. staged samples (clamped positions are what the margin holds)
+  // 1. staged samples (the margin holds the clamped values)
   for (int e = tid; e < kRegion * kRegion; e += kIntraThreads) {
     const int ly = e / kRegion - 1, lx = e % kRegion - 1;
     S.px[(ly + 1) * kRegionStride + lx + 1] = (uint8_t)at(src, oy + ly, ox + lx);
   }
   for (int e = tid; e < kBlocks * kModes; e += kIntraThreads) (&S.acc[0][0])[e] = 0;
   __syncthreads();
-  // 2. DC values (dc_value, intra_common.h:120-128)
-  for (int b = tid; b < kBlocks; b += kIntraThreads) {
+  // 2. edge arrays (edge_above / edge_left) and DC values (dc_value) per block
+  for (int b = 5 + tid; b < kBlocks; b += kIntraThreads) {
     int x, y, bw, bh;
     sb_block_geom(b, x, y, bw, bh);
-    const bool has_a = oy + y > 0, has_l = ox + x > 0;
-    int sum = 0, n = 0;
-    if (has_a)
-      for (int j = 0; j < bw; j++) sum += S.px[y * kRegionStride + x + j + 1], n++;
-    if (has_l)
-      for (int i = 0; i < bh; i++) sum += S.px[(y + i + 1) * kRegionStride + x], n++;
-    S.dc[b] = n ? (sum + n / 2) / n : 128;
+    const bool top = oy + y == 0, lft = ox + x == 0;
+    const int off = edge_offset(b), n = bw + bh;
+    auto s = [&](int ly, int lx) { return (int)S.px[(ly + 1) * kRegionStride + lx + 1]; };
+    for (int k = -1; k < n; k++) {
+      S.above[off + k + 1] = (uint8_t)(top ? 128 : (k < 0 && lft) ? s(y - 1, x) : s(y - 1, x + k));
+      S.left[off + k + 1] = (uint8_t)(lft ? 128 : (k < 0 && top) ? s(y, x - 1) : s(y + k, x - 1));
+    }
+    int sum = 0, cnt = 0;
+    if (!top)
+      for (int j = 0; j < bw; j++) sum += s(y - 1, x + j), cnt++;
+    if (!lft)
+      for (int i = 0; i < bh; i++) sum += s(y + i, x - 1), cnt++;
+    S.dc[b] = cnt ? (sum + cnt / 2) / cnt : 128;
   }
   __syncthreads();
+
   // 3. (block, tile) items: 13 predictions + Hadamards per tile, segment sums per block
   for (int base = kIntraFirst; base < kItems; base += kIntraThreads) {
-    const int item = base + tid;  // kIntraItems is a multiple of the CTA size: always valid
-    const uint32_t it = job.items[item];
-    const int b = item_block(it), width = item_width(item);
-    IntraBlock B;
-    B.px = S.px;
-    sb_block_geom(b, B.x, B.y, B.w, B.h);
-    B.top = oy + B.y == 0, B.left = ox + B.x == 0;
-    const int tx = item_tx(it) * 4, ty = item_ty(it) * 4;  // superblock-local tile origin
+    const int item = base + tid;  // the intra items are a multiple of the CTA size
+    int b, tx, ty;
+    item_decode(item, b, tx, ty);
+    const int width = item_width(item);
+    int x, y, bw, bh;
+    sb_block_geom(b, x, y, bw, bh);
+    const uint8_t* A = S.above + edge_offset(b) + 1;  // A[k], k >= -1
+    const uint8_t* L = S.left + edge_offset(b) + 1;
+    const int last = bw + bh - 1;
+    const int r0 = ty * 4 - y, c0 = tx * 4 - x;  // the tile's origin inside the block
     int cur[16];
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-      for (int j = 0; j < 4; j++) cur[4 * i + j] = B.s(ty + i, tx + j);
-    const int bi = ty - B.y, bj = tx - B.x;  // tile origin inside the block
+      for (int j = 0; j < 4; j++) cur[4 * i + j] = S.px[(ty * 4 + i + 1) * kRegionStride + tx * 4 + j + 1];
+    const int lgw = 31 - __clz(bw), lgh = 31 - __clz(bh);
+    const int den = bw + bh + 2;
+    const float rcp = 1.0f / (float)den;
 #pragma unroll 1
     for (int m = 0; m < kModes; m++) {
       int d[16];
-      if (m == 0) {
+      switch (m) {
+        case 0: {
+          const int v = S.dc[b];
 #pragma unroll
-        for (int k = 0; k < 16; k++) d[k] = cur[k] - S.dc[b];
-      } else {
+          for (int k = 0; k < 16; k++) d[k] = cur[k] - v;
+          break;
+        }
+        case 1:
 #pragma unroll
-        for (int i = 0; i < 4; i++)
+          for (int i = 0; i < 4; i++)
 #pragma unroll
-          for (int j = 0; j < 4; j++) d[4 * i + j] = cur[4 * i + j] - intra_pred(B, m, bi + i, bj + j);
+            for (int j = 0; j < 4; j++) d[4 * i + j] = cur[4 * i + j] - A[c0 + j];
+          break;
+        case 2:
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) d[4 * i + j] = cur[4 * i + j] - L[r0 + i];
+          break;
+        case 3: {  // Smooth: bilinear blend of above, left, top-right and bottom-left
+          const int tr = A[bw - 1], bl = L[bh - 1];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const int ii = r0 + i, jj = c0 + j;
+              const int num = (bh - ii) * A[jj] + (ii + 1) * bl + (bw - jj) * L[ii] + (jj + 1) * tr;
+              d[4 * i + j] = cur[4 * i + j] - exact_div(num + den / 2, den, rcp);
+            }
+          break;
+        }
+        case 4: {  // SmoothV (h is a power of two, the numerator non-negative)
+          const int bl = L[bh - 1];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const int ii = r0 + i;
+              d[4 * i + j] = cur[4 * i + j] - (((bh - 1 - ii) * A[c0 + j] + (ii + 1) * bl + bh / 2) >> lgh);
+            }
+          break;
+        }
+        case 5: {  // SmoothH
+          const int tr = A[bw - 1];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const int jj = c0 + j;
+              d[4 * i + j] = cur[4 * i + j] - (((bw - 1 - jj) * L[r0 + i] + (jj + 1) * tr + bw / 2) >> lgw);
+            }
+          break;
+        }
+        case 6: {  // Paeth
+          const int tl = A[-1];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const int a = A[c0 + j], l = L[r0 + i], bse = a + l - tl;
+              const int pa = abs(bse - a), pl = abs(bse - l), ptl = abs(bse - tl);
+              d[4 * i + j] = cur[4 * i + j] - (pl <= pa && pl <= ptl ? l : pa <= ptl ? a : tl);
+            }
+          break;
+        }
+        case 7:
+        case 8: {  // z1: D45 (derivative 64), D67 (27), from the row above
+          const int dxa = m == 7 ? 64 : 27;
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            const int pos = (r0 + i + 1) * dxa, b0 = (pos >> 6) + c0, sh = (pos & 63) >> 1;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const int p0 = A[min(b0 + j, last)], p1 = A[min(b0 + j + 1, last)];
+              d[4 * i + j] = cur[4 * i + j] - ((p0 * (32 - sh) + p1 * sh + 16) >> 5);
+            }
+          }
+          break;
+        }
+        case 12: {  // z3: D203 (derivative 27), from the column left
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const int pos = (c0 + j + 1) * 27, b0 = (pos >> 6) + r0, sh = (pos & 63) >> 1;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+              const int p0 = L[min(b0 + i, last)], p1 = L[min(b0 + i + 1, last)];
+              d[4 * i + j] = cur[4 * i + j] - ((p0 * (32 - sh) + p1 * sh + 16) >> 5);
+            }
+          }
+          break;
+        }
+        default: {  // z2: D113, D135, D157 -- the row above while the projection stays on it
+          const int dxa = m == 9 ? 27 : m == 10 ? 64 : 151, dya = m == 9 ? 151 : m == 10 ? 64 : 27;
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const int ii = r0 + i, jj = c0 + j;
+              const int px = (jj << 6) - (ii + 1) * dxa, bx = px >> 6;
+              int p;
+              if (bx >= -1) {
+                const int sh = (px & 63) >> 1;
+                p = (A[bx] * (32 - sh) + A[bx + 1] * sh + 16) >> 5;
+              } else {
+                const int py = (ii << 6) - (jj + 1) * dya, by = py >> 6, sh = (py & 63) >> 1;
+                p = (L[max(by, -1)] * (32 - sh) + L[max(by + 1, -1)] * sh + 16) >> 5;
+              }
+              d[4 * i + j] = cur[4 * i + j] - p;
+            }
+          break;
+        }
       }
       const int s = segment_sum(hadamard4x4(d), width);
       if ((tid & ((width < 32 ? width : 32) - 1)) == 0) atomicAdd(&S.acc[b][m], s);

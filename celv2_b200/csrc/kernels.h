@@ -31,7 +31,9 @@ void launch_pyramid(const DevPyramid& pyr, cudaStream_t st);
 void launch_phases(const DevPlane& lv0, cudaStream_t st);
 
 // Motion search of one pyramid level for every (job, reference, 8x8 cell); level 0 includes the
-// quarter-pel refinement. Units: nrefs * fcols[level] * frows[level] per job.
+// quarter-pel refinement. Units: me_units(nrefs, fcols[level], frows[level]) per job (groups of
+// 32 cells of one reference).
+int me_units(int nrefs, int cols, int rows);
 void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, cudaStream_t st);
 
 // Intra SATDs of every candidate block and mode. Units: sb_cols * sb_rows per job.

@@ -5,24 +5,43 @@
 // (:122-133), me_refine (:141-154), me_cell (:162-193); driven level by level, coarsest first,
 // as src/gpu/cpu_engine.cpp:68-83 does.
 //
-// One warp per (job, reference, 8x8 cell):
-//  1. the cur block is held in registers (8 rows x 2 words of packed bytes);
-//  2. lanes 0-5 compute the SADs of the six predictor centres at once; every lane then replays
-//     the reference's sequential choice of the two best distinct centres (uniform in the warp);
-//  3. per searched centre the 24 x 27-byte reference window is staged in shared memory as four
-//     byte-shifted copies, so an 8-byte row at any offset is two aligned 32-bit words; each lane
-//     takes positions lane, lane + 32, ... of the 289, sums the 8 rows with __vsadu4, and the
-//     warp reduces (cost << 9 | raster index) with a min -- which is the reference's first strict
-//     minimum in dy-major order;
-//  4. at level 0 lanes 0-8 compute the nine 8x8 quarter-pel SATDs of each refinement step and
-//     every lane replays the centre-first strict choice.
-// Integer ALU bound: per cell and centre 289 x 16 __vsadu4 on shared-memory words.
+// One CTA per 32 consecutive 8x8 cells of one (job, reference):
+//  A. the cells' cur blocks are staged in shared memory; one thread per (cell, predictor centre)
+//     computes the six centre SADs;
+//  B. one thread per cell replays the reference's sequential choice of the two best distinct
+//     centres, and the searches (one or two per cell) get their 24 x 32-byte reference windows
+//     staged in shared memory with aligned 32-bit loads;
+//  C. one thread per (search, dx) column slides down the window's 24 rows: each row's 8 bytes at
+//     column dx are loaded once (two funnel shifts of three words) and feed, with __vsadu4, every
+//     one of the 17 dy accumulators whose 8x8 block covers that row -- 24 row loads instead of
+//     17 x 8 per column. The column's best (cost << 9 | raster index) goes to a shared atomicMin,
+//     which yields the reference's first strict minimum in dy-major order;
+//  D. at level 0, the 9 positions of each refinement step are (cell, position) items computing the
+//     8x8 quarter-pel SATD from the phase planes; one thread per cell replays the centre-first
+//     strict choice.
+// Integer ALU bound: 289 x 16 __vsadu4 per searched centre.
 #include "kernels.h"
 
 namespace celv2cu {
 
-constexpr int kMeWarps = 8;
-constexpr int kWinRows = 24, kWinWords = 6;
+constexpr int kMeThreads = 256;
+constexpr int kMeCells = 32;                   // cells per CTA
+constexpr int kMeSearches = 2 * kMeCells;      // at most two centres per cell
+constexpr int kWinRows = 24, kWinWords = 8;    // a window row: 32 bytes from a 4-byte boundary
+constexpr int kWinStride = kWinRows * kWinWords + 8;  // +8 words: neighbouring windows use other banks
+
+struct MeSmem {
+  uint32_t cur[kMeCells][16];
+  int csad[kMeCells][6];
+  int ccx[kMeCells][6], ccy[kMeCells][6];
+  int scell[kMeSearches], sx[kMeSearches], sy[kMeSearches], soff[kMeSearches];
+  unsigned skey[kMeSearches];
+  int first_search[kMeCells], two[kMeCells];
+  int mvx[kMeCells], mvy[kMeCells];
+  int rsatd[kMeCells][9];
+  int nsearch;
+  uint32_t win[kMeSearches * kWinStride];
+};
 
 // 4 bytes of a plane at (x .. x + 3, y), clamped like Plane::at where the row leaves the margin.
 __device__ __forceinline__ uint32_t row4(const DevPlane& s, int x, int y) {
@@ -34,8 +53,8 @@ __device__ __forceinline__ uint32_t row4(const DevPlane& s, int x, int y) {
   return v;
 }
 
-// sad8 of the cur block (registers) against the reference at (x, y).
-__device__ __forceinline__ int sad8(const uint32_t c[16], const DevPlane& ref, int x, int y) {
+// sad8 of a cur block (shared memory) against the reference at (x, y).
+__device__ __forceinline__ int sad8(const uint32_t* c, const DevPlane& ref, int x, int y) {
   unsigned s = 0;
 #pragma unroll
   for (int i = 0; i < 8; i++) {
@@ -45,8 +64,8 @@ __device__ __forceinline__ int sad8(const uint32_t c[16], const DevPlane& ref, i
   return (int)s;
 }
 
-// satd8_q: the 8x8 SATD of the cur block against the quarter-pel prediction at (qx, qy).
-__device__ __forceinline__ int satd8_q(const uint32_t c[16], const DevPlane& ref, int x0, int y0, int qx, int qy) {
+// satd8_q: the 8x8 SATD of a cur block against the quarter-pel prediction at (qx, qy).
+__device__ __forceinline__ int satd8_q(const uint32_t* c, const DevPlane& ref, int x0, int y0, int qx, int qy) {
   DevPlane ph = ref;
   ph.p = ref.p + (long long)((qy & 3) * 4 + (qx & 3)) * ref.phase;
   const int x = x0 + (qx >> 2), y = y0 + (qy >> 2);
@@ -63,123 +82,174 @@ __device__ __forceinline__ int satd8_q(const uint32_t c[16], const DevPlane& ref
   return total;
 }
 
-__global__ void __launch_bounds__(kMeWarps * 32) k_me_level(const FrameJob* __restrict__ jobs, WorkList w, int level) {
-  __shared__ uint32_t win[kMeWarps][4][kWinRows][kWinWords];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int unit = blockIdx.x * kMeWarps + warp;
-  if (unit >= w.prefix[w.njobs]) return;  // whole warps only; no block-wide barrier below
+// The refinement step's position n (raster 0..8 with the centre, 4, visited first).
+__device__ __forceinline__ int refine_pos(int t) { return t == 0 ? 4 : (t <= 4 ? t - 1 : t); }
+
+__global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restrict__ jobs, WorkList w, int level) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  MeSmem& S = *reinterpret_cast<MeSmem*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int unit = blockIdx.x;
   const int jb = job_of(w, unit);
   const FrameJob& job = jobs[jb];
   const int cols = job.fcols[level], rows = job.frows[level], ncell = cols * rows;
+  const int groups = (ncell + kMeCells - 1) / kMeCells;
   const int u = unit - w.prefix[jb];
-  const int r = u / ncell, cell = u - r * ncell, by = cell / cols, bx = cell - by * cols;
+  const int r = u / groups, cell0 = (u - r * groups) * kMeCells;
+  const int ncells = min(kMeCells, ncell - cell0);
   const DevPlane cur = job.cur.lv[level], ref = job.ref[r].lv[level];
-  const int x0 = bx * 8, y0 = by * 8;
 
-  uint32_t c[16];
-#pragma unroll
-  for (int i = 0; i < 8; i++) c[2 * i] = row4(cur, x0, y0 + i), c[2 * i + 1] = row4(cur, x0 + 4, y0 + i);
-
-  // ---- 2. predictor centres (me_cell, inter_common.h:164-186) ----
-  int px = 0, py = 0, px2 = 0, py2 = 0;
-  bool two = false;
-  if (level < kLevels - 1) {
-    const int* pf = job.field[r][level + 1];
-    const int pcols = job.fcols[level + 1], prows = job.frows[level + 1];
-    int cx[6], cy[6];
-#pragma unroll
-    for (int k = 0; k < 6; k++) {
-      cx[k] = 0, cy[k] = 0;
+  // ---- A. cur blocks, predictor centres and their SADs (me_cell, inter_common.h:164-186) ----
+  for (int e = tid; e < kMeCells * 16; e += kMeThreads) {
+    const int c = e >> 4, k = e & 15;
+    const int cell = cell0 + (c < ncells ? c : 0), by = cell / cols, bx = cell - by * cols;
+    S.cur[c][k] = row4(cur, bx * 8 + 4 * (k & 1), by * 8 + (k >> 1));
+  }
+  if (tid == 0) S.nsearch = 0;
+  __syncthreads();
+  const bool top = level == kLevels - 1;
+  if (!top && tid < kMeCells * 6) {
+    const int c = tid / 6, k = tid - c * 6;
+    if (c < ncells) {
+      const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
+      int cx = 0, cy = 0;  // k == 5: zero
       if (k < 5) {
+        const int* pf = job.field[r][level + 1];
+        const int pcols = job.fcols[level + 1], prows = job.frows[level + 1];
         const int ox = k == 1 ? -1 : k == 2 ? 1 : 0, oy = k == 3 ? -1 : k == 4 ? 1 : 0;
-        const int qx = clampi(bx / 2 + ox, 0, pcols - 1), qy = clampi(by / 2 + oy, 0, prows - 1);
-        const int m = pf[qy * pcols + qx];
-        cx[k] = 2 * mv_x(m), cy[k] = 2 * mv_y(m);
+        const int m = pf[clampi(by / 2 + oy, 0, prows - 1) * pcols + clampi(bx / 2 + ox, 0, pcols - 1)];
+        cx = 2 * mv_x(m), cy = 2 * mv_y(m);
       }
-    }
-    int mine = 0;
-#pragma unroll
-    for (int k = 0; k < 6; k++)
-      if (lane == k) mine = sad8(c, ref, x0 + cx[k], y0 + cy[k]);
-    int best = 0x7fffffff, second = 0x7fffffff;
-#pragma unroll
-    for (int k = 0; k < 6; k++) {
-      const int s = __shfl_sync(0xffffffffu, mine, k);
-      if ((k > 0 && cx[k] == px && cy[k] == py) || (two && cx[k] == px2 && cy[k] == py2)) continue;
-      if (s < best) {
-        if (k > 0) second = best, px2 = px, py2 = py, two = true;
-        best = s, px = cx[k], py = cy[k];
-      } else if (s < second) {
-        second = s, px2 = cx[k], py2 = cy[k], two = true;
-      }
+      S.ccx[c][k] = cx, S.ccy[c][k] = cy;
+      S.csad[c][k] = sad8(S.cur[c], ref, bx * 8 + cx, by * 8 + cy);
     }
   }
+  __syncthreads();
 
-  // ---- 3. +-8 search around each centre (me_search, inter_common.h:108-119) ----
-  uint32_t(*W)[kWinRows][kWinWords] = win[warp];
-  auto search = [&](int cxs, int cys) -> unsigned {
-    const int wx0 = x0 + cxs - kMeRange, wy0 = y0 + cys - kMeRange;
-    __syncwarp();
-    for (int e = lane; e < 4 * kWinRows * kWinWords; e += 32) {
-      const int s = e / (kWinRows * kWinWords), rem = e - s * (kWinRows * kWinWords);
-      const int rr = rem / kWinWords, ww = rem - rr * kWinWords;
-      W[s][rr][ww] = row4(ref, wx0 + 4 * ww + s, wy0 + rr);
+  // ---- B. the two best distinct centres per cell, the search list ----
+  if (tid < ncells) {
+    const int c = tid;
+    int px = 0, py = 0, px2 = 0, py2 = 0;
+    bool two = false;
+    if (!top) {
+      int best = 0x7fffffff, second = 0x7fffffff;
+      for (int k = 0; k < 6; k++) {
+        const int cx = S.ccx[c][k], cy = S.ccy[c][k], s = S.csad[c][k];
+        if ((k > 0 && cx == px && cy == py) || (two && cx == px2 && cy == py2)) continue;
+        if (s < best) {
+          if (k > 0) second = best, px2 = px, py2 = py, two = true;
+          best = s, px = cx, py = cy;
+        } else if (s < second) {
+          second = s, px2 = cx, py2 = cy, two = true;
+        }
+      }
     }
-    __syncwarp();
-    unsigned best = 0xffffffffu;
-    for (int idx = lane; idx < 289; idx += 32) {
-      const int dyi = idx / 17, dxi = idx - dyi * 17;
-      const int s = dxi & 3, wo = dxi >> 2;
-      unsigned sad = 0;
+    const int s0 = atomicAdd(&S.nsearch, two ? 2 : 1);
+    S.first_search[c] = s0, S.two[c] = two;
+    const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
+    for (int k = 0; k < (two ? 2 : 1); k++) {
+      const int cxs = k ? px2 : px, cys = k ? py2 : py;
+      const int wx0 = bx * 8 + cxs - kMeRange;
+      S.scell[s0 + k] = c, S.sx[s0 + k] = cxs, S.sy[s0 + k] = cys;
+      S.soff[s0 + k] = wx0 - (wx0 & ~3);  // the window starts on the 4-byte boundary below wx0
+      S.skey[s0 + k] = 0xffffffffu;
+    }
+  }
+  __syncthreads();
+  const int nsearch = S.nsearch;
+  // windows: rows y0 + cy - 8 .. + 23, 8 words from the 4-byte boundary at or below x0 + cx - 8
+  for (int e = tid; e < nsearch * kWinRows * kWinWords; e += kMeThreads) {
+    const int s = e / (kWinRows * kWinWords), rem = e - s * (kWinRows * kWinWords);
+    const int rr = rem >> 3, ww = rem & 7;
+    const int cell = cell0 + S.scell[s], by = cell / cols, bx = cell - by * cols;
+    const int wx = ((bx * 8 + S.sx[s] - kMeRange) & ~3) + 4 * ww, wy = by * 8 + S.sy[s] - kMeRange + rr;
+    S.win[s * kWinStride + rr * kWinWords + ww] = row4(ref, wx, wy);
+  }
+  __syncthreads();
+
+  // ---- C. +-8 search (me_search, inter_common.h:108-119): a thread per (search, dx) ----
+  for (int item = tid; item < nsearch * 17; item += kMeThreads) {
+    const int s = item / 17, dx = item - s * 17;
+    const uint32_t* c = S.cur[S.scell[s]];
+    uint32_t cw[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) cw[k] = c[k];
+    const int b = S.soff[s] + dx, wi = b >> 2;
+    const unsigned sh = (unsigned)(b & 3) * 8;
+    const uint32_t* wr = S.win + s * kWinStride + wi;
+    unsigned acc[17];
+#pragma unroll
+    for (int k = 0; k < 17; k++) acc[k] = 0;
+#pragma unroll
+    for (int rr = 0; rr < kWinRows; rr++) {
+      const uint32_t u0 = wr[rr * kWinWords], u1 = wr[rr * kWinWords + 1], u2 = wr[rr * kWinWords + 2];
+      const uint32_t w0 = __funnelshift_r(u0, u1, sh), w1 = __funnelshift_r(u1, u2, sh);
 #pragma unroll
       for (int i = 0; i < 8; i++) {
-        sad = __vsadu4(c[2 * i], W[s][dyi + i][wo]) + sad;
-        sad = __vsadu4(c[2 * i + 1], W[s][dyi + i][wo + 1]) + sad;
+        const int dy = rr - i;
+        if (dy >= 0 && dy <= 16) acc[dy] = __vsadu4(cw[2 * i + 1], w1) + (__vsadu4(cw[2 * i], w0) + acc[dy]);
       }
-      const unsigned cost = sad + kMePenalty * (abs(dxi - kMeRange) + abs(dyi - kMeRange));
-      const unsigned key = (cost << 9) | (unsigned)idx;
+    }
+    unsigned best = 0xffffffffu;
+    const unsigned pen_x = kMePenalty * abs(dx - kMeRange);
+#pragma unroll
+    for (int dy = 0; dy < 17; dy++) {
+      const unsigned cost = acc[dy] + pen_x + kMePenalty * abs(dy - kMeRange);
+      const unsigned key = (cost << 9) | (unsigned)(dy * 17 + dx);
       best = key < best ? key : best;
     }
-    return __reduce_min_sync(0xffffffffu, best);
-  };
-  unsigned k1 = search(px, py);
-  int mx = px + (int)(k1 & 511) % 17 - kMeRange, my = py + (int)(k1 & 511) / 17 - kMeRange;
-  if (two) {
-    const unsigned k2 = search(px2, py2);
-    if ((k2 >> 9) < (k1 >> 9)) mx = px2 + (int)(k2 & 511) % 17 - kMeRange, my = py2 + (int)(k2 & 511) / 17 - kMeRange;
+    atomicMin(&S.skey[s], best);
   }
-
-  // ---- 4. quarter-pel refinement at level 0 (me_refine, inter_common.h:141-154) ----
-  if (level == 0) {
-    int cxq = mx * 4, cyq = my * 4;
-    for (int step = 2; step >= 1; step--) {
-      int mine = 0;
-      if (lane < 9) {
-        const int n = lane == 0 ? 4 : (lane <= 4 ? lane - 1 : lane);  // raster 0..8, centre (4) first
-        const int dx = n % 3 - 1, dy = n / 3 - 1;
-        mine = satd8_q(c, ref, x0, y0, cxq + dx * step, cyq + dy * step);
-      }
-      int best = __shfl_sync(0xffffffffu, mine, 0), nx = cxq, ny = cyq;
-#pragma unroll
-      for (int t = 1; t < 9; t++) {
-        const int s = __shfl_sync(0xffffffffu, mine, t) + kSubpelPenalty;
-        const int n = t <= 4 ? t - 1 : t;
-        if (s < best) best = s, nx = cxq + (n % 3 - 1) * step, ny = cyq + (n / 3 - 1) * step;
-      }
-      cxq = nx, cyq = ny;
+  __syncthreads();
+  if (tid < ncells) {
+    const int s0 = S.first_search[tid];
+    const unsigned k1 = S.skey[s0];
+    int mx = S.sx[s0] + (int)(k1 & 511) % 17 - kMeRange, my = S.sy[s0] + (int)(k1 & 511) / 17 - kMeRange;
+    if (S.two[tid]) {  // the second centre's result only if strictly cheaper (me_cell, :189-192)
+      const unsigned k2 = S.skey[s0 + 1];
+      if ((k2 >> 9) < (k1 >> 9)) mx = S.sx[s0 + 1] + (int)(k2 & 511) % 17 - kMeRange, my = S.sy[s0 + 1] + (int)(k2 & 511) / 17 - kMeRange;
     }
-    mx = cxq, my = cyq;
+    S.mvx[tid] = level == 0 ? mx * 4 : mx, S.mvy[tid] = level == 0 ? my * 4 : my;
   }
-  if (lane == 0) {
-    job.field[r][level][cell] = pack_mv(mx, my);
-    if (job.stats) atomicAdd(job.stats + level, two ? 2ull : 1ull);
+  __syncthreads();
+
+  // ---- D. quarter-pel refinement at level 0 (me_refine, inter_common.h:141-154) ----
+  if (level == 0) {
+    for (int step = 2; step >= 1; step--) {
+      for (int item = tid; item < ncells * 9; item += kMeThreads) {
+        const int c = item / 9, t = item - c * 9, n = refine_pos(t);
+        const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
+        S.rsatd[c][t] = satd8_q(S.cur[c], ref, bx * 8, by * 8, S.mvx[c] + (n % 3 - 1) * step, S.mvy[c] + (n / 3 - 1) * step);
+      }
+      __syncthreads();
+      if (tid < ncells) {
+        const int cx = S.mvx[tid], cy = S.mvy[tid];
+        int best = S.rsatd[tid][0], nx = cx, ny = cy;
+        for (int t = 1; t < 9; t++) {
+          const int s = S.rsatd[tid][t] + kSubpelPenalty, n = refine_pos(t);
+          if (s < best) best = s, nx = cx + (n % 3 - 1) * step, ny = cy + (n / 3 - 1) * step;
+        }
+        S.mvx[tid] = nx, S.mvy[tid] = ny;
+      }
+      __syncthreads();
+    }
+  }
+  if (tid < ncells) {
+    job.field[r][level][cell0 + tid] = pack_mv(S.mvx[tid], S.mvy[tid]);
+    if (job.stats) atomicAdd(job.stats + level, S.two[tid] ? 2ull : 1ull);
   }
 }
+
+int me_units(int nrefs, int cols, int rows) { return nrefs * ((cols * rows + kMeCells - 1) / kMeCells); }
 
 void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, cudaStream_t st) {
   const int units = w.prefix[w.njobs];
   if (units <= 0) return;
-  k_me_level<<<(units + kMeWarps - 1) / kMeWarps, kMeWarps * 32, 0, st>>>(jobs, w, level);
+  k_me_level<<<units, kMeThreads, sizeof(MeSmem), st>>>(jobs, w, level);
+}
+
+cudaError_t me_attributes() {
+  return cudaFuncSetAttribute(k_me_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MeSmem));
 }
 
 }  // namespace celv2cu
