@@ -155,11 +155,13 @@ def dist_setup(gpus: int):
 
 
 def max_over_ranks(v: float, dist, local: int) -> float:
+    """The max of v over all ranks (a CUDA tensor under NCCL, a CPU tensor under gloo)."""
     if dist is None:
         return v
     import torch
 
-    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+    dev = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -168,8 +170,11 @@ def barrier(dist, local):
     if dist is not None:
         import torch
 
-        dist.barrier(device_ids=[local])
-        torch.cuda.synchronize(local)
+        if dist.get_backend() == "nccl":
+            dist.barrier(device_ids=[local])
+            torch.cuda.synchronize(local)
+        else:
+            dist.barrier()
 
 
 # ---------------------------------------------------------------- the reference's CPU engine
