@@ -30,6 +30,7 @@
 #include "tables.h"
 
 namespace celv2cu {
+void set_last_error(const std::string& msg);
 cudaError_t measure_int_peak(int device, double* ops_per_s);
 cudaError_t me_attributes();
 cudaError_t inter_attributes();
@@ -40,8 +41,13 @@ cudaError_t finalize_attributes();
 using namespace celv2cu;
 
 namespace {
-
 thread_local std::string g_error;
+}  // namespace
+
+// The calling thread's message for celv2_last_error (entry points outside this file set it too).
+void celv2cu::set_last_error(const std::string& msg) { g_error = msg; }
+
+namespace {
 
 struct Error : std::runtime_error {
   int code;

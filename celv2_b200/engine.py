@@ -64,6 +64,8 @@ SIGNATURES = {
     "celv2_stage_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_int]),
     "celv2_int_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "celv2_work_counters": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int]),
+    "celv2_decide_key_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_void_p,
+                                           C.c_void_p]),
 }
 
 STAGE_NAMES = ["upload+pyramid", "phases", "me_l4", "me_l3", "me_l2", "me_l1", "me_l0", "intra", "inter",

@@ -105,6 +105,20 @@ int celv2_group_records(celv2_engine* e, int job, const celv2_sb_out** records);
 /* Drops every frame of the store. */
 int celv2_clear_store(celv2_engine* e);
 
+/* ---- A KEY-frame decision that allocates nothing ----
+ * No counterpart in the reference. For callers that cannot allocate device memory while they run
+ * (a host application that provisions all GPU memory up front, a path that cannot take the device
+ * synchronisation of cudaMalloc / cudaFree): decides an intra-only frame from the caller's padded
+ * 8-bit luma plane (`luma`, device memory, pw x ph with row pitch `pitch` >= pw) into the caller's
+ * sb_cols * sb_rows records (`out`, device memory), on `stream` (a cudaStream_t, NULL: the default
+ * stream), with the same records as celv2_launch with no references. Its scratch is a fixed static
+ * device array: frames above CELV2_NOALLOC_MAX_SUPERBLOCKS superblocks are rejected (CELV2_EINVAL);
+ * the first call on a device sets it up (call it before any stream capture); calls whose GPU work
+ * overlaps race on the shared scratch. */
+#define CELV2_NOALLOC_MAX_SUPERBLOCKS 768
+int celv2_decide_key_noalloc(const uint8_t* luma, int width, int height, int pitch, int64_t lambda_q8,
+                             celv2_sb_out* out, void* stream);
+
 /* ---- Inspection (tests) ---- */
 
 /* The last launch's motion field of reference r at pyramid level l: cols x rows packed MVs
