@@ -113,6 +113,38 @@ __device__ __forceinline__ int hadamard4x4(int d[16]) {
   return sum;
 }
 
+// Columns 0 and 2 (even) or 1 and 3 (odd) of a 4-byte row as two 16-bit lanes.
+__device__ __forceinline__ uint32_t bytes_even(uint32_t w) { return __byte_perm(w, 0, 0x4240); }
+__device__ __forceinline__ uint32_t bytes_odd(uint32_t w) { return __byte_perm(w, 0, 0x4341); }
+
+// hadamard4x4 of the byte residuals cur - pred of a 4x4 tile, rows as packed bytes: cur rows given
+// as their even / odd lanes (ce, co), prediction rows p. Each row's columns 0/2 and 1/3 ride as two
+// 16-bit lanes of one 32-bit integer, held as lo + hi * 65536 with |lo|, |hi| <= 2040 so plain
+// 32-bit adds are exact; three of the four butterfly stages run on both lanes at once, and the
+// last one with the absolute values folds into |x + y| + |x - y| = 2 max(|x|, |y|). The same sum
+// of 16 absolute Walsh-Hadamard coefficients as hadamard4x4.
+__device__ __forceinline__ int satd4_bytes(const uint32_t* ce, const uint32_t* co, const uint32_t* p) {
+  int A[4], B[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int e = (int)(ce[i] - bytes_even(p[i])), o = (int)(co[i] - bytes_odd(p[i]));
+    A[i] = e + o, B[i] = e - o;
+  }
+  int sum = 0;
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int* X = h ? B : A;
+    const int s01 = X[0] + X[1], d01 = X[0] - X[1], s23 = X[2] + X[3], d23 = X[2] - X[3];
+    const int v[4] = {s01 + s23, d01 + d23, s01 - s23, d01 - d23};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int lo = (int)(short)(v[k] & 0xffff), hi = (v[k] - lo) >> 16;
+      sum += max(abs(lo), abs(hi));
+    }
+  }
+  return 2 * sum;
+}
+
 // Residual of one 4x4 row: four cur bytes minus four prediction bytes.
 __device__ __forceinline__ void residual_row(int* d, uint32_t c, uint32_t p) {
   d[0] = (int)(c & 255) - (int)(p & 255);

@@ -98,19 +98,36 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(const FrameJob* __rest
       const int width = item_width(item);
       int s = 0;
       if (S.comp_a[b] >= 0) {  // uniform over the block's segment
-        const DevPlane r0 = job.ref[S.comp_a[b]].lv[0], r1 = job.ref[S.comp_b[b]].lv[0];
         const int m0 = S.comp_mv0[b], m1 = S.comp_mv1[b];
-        const int x = ox + tx * 4, y = oy + ty * 4;
         const int mx0 = mv_x(m0), my0 = mv_y(m0), mx1 = mv_x(m1), my1 = mv_y(m1);
-        int d[16];
+        DevPlane p0 = job.ref[S.comp_a[b]].lv[0], p1 = job.ref[S.comp_b[b]].lv[0];
+        p0.p += (long long)((my0 & 3) * 4 + (mx0 & 3)) * p0.phase;
+        p1.p += (long long)((my1 & 3) * 4 + (mx1 & 3)) * p1.phase;
+        const int x = ox + tx * 4, y = oy + ty * 4;
+        const int x0 = x + (mx0 >> 2), y0 = y + (my0 >> 2), x1 = x + (mx1 >> 2), y1 = y + (my1 >> 2);
+        if (inside(p0, x0, y0, 4, 4) && inside(p1, x1, y1, 4, 4)) {
+          uint32_t ce[4], co[4], pr[4];
 #pragma unroll
-        for (int i = 0; i < 4; i++)
-#pragma unroll
-          for (int j = 0; j < 4; j++) {
-            const int p = (at_q(r0, y + i, x + j, my0, mx0) + at_q(r1, y + i, x + j, my1, mx1) + 1) >> 1;
-            d[4 * i + j] = at(cur, y + i, x + j) - p;
+          for (int i = 0; i < 4; i++) {
+            const uint32_t c = load4(cur.p + (long long)(y + i) * cur.stride + x);
+            const uint32_t a = load4(p0.p + (long long)(y0 + i) * p0.stride + x0);
+            const uint32_t q = load4(p1.p + (long long)(y1 + i) * p1.stride + x1);
+            ce[i] = bytes_even(c), co[i] = bytes_odd(c);
+            pr[i] = __vavgu4(a, q);  // per byte (a + q + 1) >> 1
           }
-        s = hadamard4x4(d);
+          s = satd4_bytes(ce, co, pr);
+        } else {
+          const DevPlane r0 = job.ref[S.comp_a[b]].lv[0], r1 = job.ref[S.comp_b[b]].lv[0];
+          int d[16];
+#pragma unroll
+          for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const int pr = (at_q(r0, y + i, x + j, my0, mx0) + at_q(r1, y + i, x + j, my1, mx1) + 1) >> 1;
+              d[4 * i + j] = at(cur, y + i, x + j) - pr;
+            }
+          s = hadamard4x4(d);
+        }
       }
       s = segment_sum(s, width);
       if ((tid & ((width < 32 ? width : 32) - 1)) == 0 && S.comp_a[b] >= 0) atomicAdd(&S.comp_sum[b], s);

@@ -9,109 +9,124 @@
 // Work reuse: a block's SATD at an MV is the sum of its 4x4 tiles' SATDs at that MV (the blocks'
 // tiles all sit on the superblock's 4x4 grid), and every candidate MV of a superblock's blocks is
 // the level-0 MV of one of the 10 x 10 cells around it. So one CTA per (superblock, reference):
-//  1. gathers those 100 MVs (clamped into the field) and their distinct set D;
-//  2. computes, for every 8x8 cell and every MV of D, the SATDs of the cell's four 4x4 tiles and
-//     keeps the cell's top / bottom / left / right halves (2 tiles each) -- 256 |D| Hadamards
-//     instead of up to 68,352 for the blocks one by one;
-//  3. sums them into 16x16, 32x32 and 64x64 squares;
-//  4. gives every block its candidates in the reference's order, skips repeats with a per-block
-//     seen-set over D, and reads each candidate's SATD with one or two shared-memory loads.
-// The result per (block, reference) is the winning SATD and MV; the lambda terms are added by
-// the finalize stage, which alone needs the costs.
+//  1. gathers those 100 MVs (clamped into the field) and their distinct set D, and lists every
+//     block's candidates as distinct MVs in first-occurrence order (repeats dropped);
+//  2. for chunks of D: one thread per 4x4 tile (its cur samples in registers) computes the tile's
+//     SATD at every MV of the chunk -- a warp reads two contiguous image rows per load -- and the
+//     four tiles of an 8x8 cell, which sit in one warp, sum by shuffles; then the 16x16 sums;
+//  3. every (block, list position) slot of the chunk's MVs takes its SATD from those sums and a
+//     shared atomicMin of (SATD << 7 | position) keeps each block's least; position order is the
+//     candidates' order, so this is the first strict minimum of the reference's loop.
+// 256 |D| Hadamards per (superblock, reference) instead of up to 68,352 for the blocks one by one.
+// The result per (block, reference) is the winning SATD and MV; the lambda terms are added by the
+// finalize stage, which alone needs the costs.
 #include "kernels.h"
 
 namespace celv2cu {
 
-constexpr int kInterThreads = 256;
-constexpr int kNb = 100;  // 10 x 10 cells around the superblock
+constexpr int kInterThreads = 256;  // one per 4x4 tile of the superblock
+constexpr int kNb = 100;            // 10 x 10 cells around the superblock
+constexpr int kChunk = 64;          // distinct MVs per pass at most
+constexpr int kSlots = 4296;        // candidates of the 425 blocks (cells covered + 8 neighbours)
 
-// The SATD of the 8x8 cell at (x, y) against phase plane `ph` at whole-pel offset (mx, my):
-// its top, bottom, left and right halves (two 4x4 Hadamards each).
-__device__ __forceinline__ void cell_halves(const uint32_t c[16], const DevPlane& ph, int x, int y, int& top, int& bot,
-                                            int& lft, int& rgt) {
-  int t[4];
-  const bool in = inside(ph, x, y, 8, 8);
-  const uint8_t* p = ph.p + (long long)y * ph.stride + x;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int tx = q & 1, ty = q >> 1;
-    int d[16];
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-      uint32_t pr;
-      if (in) {
-        pr = load4(p + (long long)(4 * ty + i) * ph.stride + 4 * tx);
-      } else {
-        pr = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) pr |= (uint32_t)at(ph, y + 4 * ty + i, x + 4 * tx + k) << (8 * k);
-      }
-      residual_row(d + 4 * i, c[2 * (4 * ty + i) + tx], pr);
-    }
-    t[q] = hadamard4x4(d);
-  }
-  top = t[0] + t[1], bot = t[2] + t[3], lft = t[0] + t[2], rgt = t[1] + t[3];
-}
+// Where block b's candidate list starts (blocks in index order, mv_candidates() slots each), and
+// for every slot its block and list position (b | position << 9).
+__constant__ short c_slot_off[kBlocks];
+__device__ unsigned short g_slot[kSlots];
 
 struct InterSmem {
-  int nb[kNb];         // packed MV of each neighbourhood cell
-  unsigned char dmap[kNb];
-  int D[kNb];          // distinct MVs
-  int nd;
+  int nb[kNb];  // packed MV of each neighbourhood cell
+  int D[kNb];   // distinct MVs, first occurrence order
   int first_idx[kNb];
-  ushort4 halves[kNb][64];  // per d, per 8x8 cell: top, bottom, left, right
-  int sum16[kNb][16];
-  int sum32[kNb][4];
-  int sum64[kNb];
-  unsigned seen[kInterThreads][4];
+  unsigned char dmap[kNb];
+  unsigned char nlist[kBlocks];
+  unsigned char list[kSlots];         // per block: its candidates' distinct MVs, first occurrence order
+  unsigned key[kBlocks];              // per block: least (SATD << 7 | position) so far
+  unsigned short tile[kChunk][256];   // 4x4 SATDs (at most 16 x 4 x 255 = 16,320)
+  unsigned short whole8[kChunk][64];  // 8x8 sums (at most 65,280)
+  int sum16[kChunk][16];
+  int nd;
 };
 
-// SATD of block b at distinct MV d from the shared sums.
-__device__ __forceinline__ int block_satd(const InterSmem& S, int b, int d) {
+// SATD of block b at chunk-local MV dd from the shared sums.
+__device__ __forceinline__ int block_satd(const InterSmem& S, int b, int dd) {
   const int sq = b / 5, kind = b - sq * 5;
-  auto whole8 = [&](int cx, int cy) {
-    const ushort4 h = S.halves[d][cy * 8 + cx];
-    return (int)h.x + (int)h.y;
-  };
-  if (sq >= 21) {  // 8x8
-    const ushort4 h = S.halves[d][sq - 21];
-    return kind == 0 ? (int)h.x + (int)h.y : kind == 1 ? (int)h.x : kind == 2 ? (int)h.y : kind == 3 ? (int)h.z : (int)h.w;
+  if (sq >= 21) {  // 8x8 cell c: its tiles t, t + 1, t + 16, t + 17
+    const int c = sq - 21, t = (c >> 3) * 32 + (c & 7) * 2;
+    const unsigned short* T = S.tile[dd];
+    switch (kind) {
+      case 0: return S.whole8[dd][c];
+      case 1: return T[t] + T[t + 1];
+      case 2: return T[t + 16] + T[t + 17];
+      case 3: return T[t] + T[t + 16];
+      default: return T[t + 1] + T[t + 17];
+    }
   }
   if (sq >= 5) {  // 16x16: children are 8x8 cells
-    const int i = sq - 5, qx = i & 3, qy = i >> 2, cx = 2 * qx, cy = 2 * qy;
+    const int i = sq - 5, c = (i >> 2) * 16 + (i & 3) * 2;
+    const unsigned short* W = S.whole8[dd];
     switch (kind) {
-      case 0: return S.sum16[d][i];
-      case 1: return whole8(cx, cy) + whole8(cx + 1, cy);
-      case 2: return whole8(cx, cy + 1) + whole8(cx + 1, cy + 1);
-      case 3: return whole8(cx, cy) + whole8(cx, cy + 1);
-      default: return whole8(cx + 1, cy) + whole8(cx + 1, cy + 1);
+      case 0: return S.sum16[dd][i];
+      case 1: return W[c] + W[c + 1];
+      case 2: return W[c + 8] + W[c + 9];
+      case 3: return W[c] + W[c + 8];
+      default: return W[c + 1] + W[c + 9];
     }
   }
+  const int* s = S.sum16[dd];
   if (sq >= 1) {  // 32x32: children are 16x16 squares
-    const int i = sq - 1, qx = i & 1, qy = i >> 1, c0 = (2 * qy) * 4 + 2 * qx;
-    const int* s = S.sum16[d];
+    const int i = sq - 1, c0 = (i >> 1) * 8 + (i & 1) * 2;
+    const int tl = s[c0], tr = s[c0 + 1], bl = s[c0 + 4], br = s[c0 + 5];
     switch (kind) {
-      case 0: return S.sum32[d][i];
-      case 1: return s[c0] + s[c0 + 1];
-      case 2: return s[c0 + 4] + s[c0 + 5];
-      case 3: return s[c0] + s[c0 + 4];
-      default: return s[c0 + 1] + s[c0 + 5];
+      case 0: return tl + tr + bl + br;
+      case 1: return tl + tr;
+      case 2: return bl + br;
+      case 3: return tl + bl;
+      default: return tr + br;
     }
   }
-  const int* s = S.sum32[d];
+  int q[4];  // the 32x32 quadrants
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int c0 = (i >> 1) * 8 + (i & 1) * 2;
+    q[i] = s[c0] + s[c0 + 1] + s[c0 + 4] + s[c0 + 5];
+  }
   switch (kind) {
-    case 0: return S.sum64[d];
-    case 1: return s[0] + s[1];
-    case 2: return s[2] + s[3];
-    case 3: return s[0] + s[2];
-    default: return s[1] + s[3];
+    case 0: return q[0] + q[1] + q[2] + q[3];
+    case 1: return q[0] + q[1];
+    case 2: return q[2] + q[3];
+    case 3: return q[0] + q[2];
+    default: return q[1] + q[3];
   }
 }
 
-__global__ void __launch_bounds__(kInterThreads, 2) k_inter(const FrameJob* __restrict__ jobs, WorkList w) {
+// Neighbourhood index (10 x 10, origin one cell above-left of the superblock) of candidate k of
+// the block at superblock-local (bx, by), size bw x bh (candidate_mv_index, inter_common.h:65-78).
+__device__ __forceinline__ int candidate_cell(int bx, int by, int bw, int bh, int k) {
+  const int lx = bx >> 3, ly = by >> 3;
+  const int cw = ((bx + bw - 1) >> 3) - lx + 1, ch = ((by + bh - 1) >> 3) - ly + 1, cells = cw * ch;
+  int cx, cy;
+  if (k < cells) {
+    const int kr = k / cw;
+    cx = lx + (k - kr * cw), cy = ly + kr;
+  } else {
+    const int n = k - cells;
+    const int nl = lx - 1, nr = (bx + bw) >> 3, nt = ly - 1, nbm = (by + bh) >> 3;
+    cx = (n == 0 || n == 4 || n == 6) ? nl : (n == 2 || n == 5 || n == 7) ? nr : lx;
+    cy = (n == 1 || n == 4 || n == 5) ? nt : (n == 3 || n == 6 || n == 7) ? nbm : ly;
+  }
+  return (cy + 1) * 10 + cx + 1;
+}
+
+__device__ __forceinline__ int mv_candidates(int bx, int by, int bw, int bh) {
+  return (((bx + bw - 1) >> 3) - (bx >> 3) + 1) * (((by + bh - 1) >> 3) - (by >> 3) + 1) + 8;
+}
+
+__global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __restrict__ jobs, WorkList w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   InterSmem& S = *reinterpret_cast<InterSmem*>(smem_raw);
-  const int tid = threadIdx.x;
+  __shared__ int warp_cnt[kInterThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31;
   const int unit = blockIdx.x;
   const int jb = job_of(w, unit);
   const FrameJob& job = jobs[jb];
@@ -122,12 +137,13 @@ __global__ void __launch_bounds__(kInterThreads, 2) k_inter(const FrameJob* __re
   const int cols = job.fcols[0], rows = job.frows[0];
   const int* field = job.field[r][0];
 
-  // 1. neighbourhood MVs and their distinct set (first occurrence order)
+  // 1. neighbourhood MVs, their distinct set (first occurrence order), the blocks' lists
   if (tid < kNb) {
     const int ny = tid / 10, nx = tid - ny * 10;
     const int cx = clampi(sbx * 8 - 1 + nx, 0, cols - 1), cy = clampi(sby * 8 - 1 + ny, 0, rows - 1);
     S.nb[tid] = field[cy * cols + cx];
   }
+  for (int b = tid; b < kBlocks; b += kInterThreads) S.key[b] = 0xffffffffu;
   __syncthreads();
   bool is_first = false;
   int firstj = 0;
@@ -136,97 +152,112 @@ __global__ void __launch_bounds__(kInterThreads, 2) k_inter(const FrameJob* __re
     while (S.nb[firstj] != v) firstj++;
     is_first = firstj == tid;
   }
-  // prefix count of first occurrences (4 warps cover the 100 entries)
   const unsigned bal = __ballot_sync(0xffffffffu, is_first);
-  __shared__ int warp_cnt[kInterThreads / 32];
-  if ((tid & 31) == 0) warp_cnt[tid >> 5] = __popc(bal);
+  if (lane == 0) warp_cnt[tid >> 5] = __popc(bal);
   __syncthreads();
   if (tid < kNb) {
-    int pos = __popc(bal & ((1u << (tid & 31)) - 1u));
+    int pos = __popc(bal & ((1u << lane) - 1u));
     for (int k = 0; k < (tid >> 5); k++) pos += warp_cnt[k];
     if (is_first) S.D[pos] = S.nb[tid], S.first_idx[tid] = pos;
   }
-  if (tid == 0) {
-    int n = 0;
-    for (int k = 0; k < (kNb + 31) / 32; k++) n += warp_cnt[k];
-    S.nd = n;
-  }
+  if (tid == 0) S.nd = warp_cnt[0] + warp_cnt[1] + warp_cnt[2] + warp_cnt[3];
   __syncthreads();
   if (tid < kNb) S.dmap[tid] = (unsigned char)S.first_idx[firstj];
   const int nd = S.nd;
   if (tid == 0 && job.stats) atomicAdd(job.stats + kStatInterMvs, (unsigned long long)nd);
-
-  // 2. per 8x8 cell and distinct MV: the tile SATD halves
-  {
-    const int cell = tid & 63, cx = cell & 7, cy = cell >> 3;
-    const DevPlane cur = job.cur.lv[0];
-    const DevPlane ref = job.ref[r].lv[0];
-    const int x = ox + cx * 8, y = oy + cy * 8;
-    uint32_t c[16];
-#pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const uint8_t* p = cur.p + (long long)(y + i) * cur.stride + x;
-      c[2 * i] = load4(p), c[2 * i + 1] = load4(p + 4);  // the SB grid lies inside the cur margin
-    }
-    for (int d = tid >> 6; d < nd; d += kInterThreads / 64) {
-      const int m = S.D[d], mx = mv_x(m), my = mv_y(m);
-      DevPlane ph = ref;
-      ph.p = ref.p + (long long)((my & 3) * 4 + (mx & 3)) * ref.phase;
-      int t, b, l, rr;
-      cell_halves(c, ph, x + (mx >> 2), y + (my >> 2), t, b, l, rr);
-      S.halves[d][cell] = make_ushort4((unsigned short)t, (unsigned short)b, (unsigned short)l, (unsigned short)rr);
-    }
-  }
   __syncthreads();
-  // 3. 16x16, 32x32, 64x64 sums
-  for (int e = tid; e < nd * 16; e += kInterThreads) {
-    const int d = e >> 4, i = e & 15, cx = 2 * (i & 3), cy = 2 * (i >> 2);
-    int s = 0;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const ushort4 h = S.halves[d][(cy + (q >> 1)) * 8 + cx + (q & 1)];
-      s += (int)h.x + (int)h.y;
-    }
-    S.sum16[d][i] = s;
-  }
-  __syncthreads();
-  for (int e = tid; e < nd * 4; e += kInterThreads) {
-    const int d = e >> 2, i = e & 3, c0 = (2 * (i >> 1)) * 4 + 2 * (i & 1);
-    S.sum32[d][i] = S.sum16[d][c0] + S.sum16[d][c0 + 1] + S.sum16[d][c0 + 4] + S.sum16[d][c0 + 5];
-  }
-  __syncthreads();
-  for (int d = tid; d < nd; d += kInterThreads) S.sum64[d] = S.sum32[d][0] + S.sum32[d][1] + S.sum32[d][2] + S.sum32[d][3];
-  __syncthreads();
-
-  // 4. every block's candidates in order (repeats skipped), first strict minimum
-  int2* out = job.inter + ((long long)sb * kMaxRefs + r) * kBlocks;
-  unsigned* seen = S.seen[tid];
   for (int b = tid; b < kBlocks; b += kInterThreads) {
     int bx, by, bw, bh;
     sb_block_geom(b, bx, by, bw, bh);
-    seen[0] = seen[1] = seen[2] = seen[3] = 0;
-    const int lx = bx >> 3, ly = by >> 3;
-    const int cw = ((bx + bw - 1) >> 3) - lx + 1, ch = ((by + bh - 1) >> 3) - ly + 1, cells = cw * ch;
-    const int nl = lx - 1, nr = (bx + bw) >> 3, nt = ly - 1, nbm = (by + bh) >> 3;
-    int best = 0x7fffffff, bestd = 0;
-    for (int k = 0; k < cells + 8; k++) {
-      int cx, cy;
-      if (k < cells) {
-        const int kr = k / cw;
-        cx = lx + (k - kr * cw), cy = ly + kr;
-      } else {
-        const int n = k - cells;
-        cx = (n == 0 || n == 4 || n == 6) ? nl : (n == 2 || n == 5 || n == 7) ? nr : lx;
-        cy = (n == 1 || n == 4 || n == 5) ? nt : (n == 3 || n == 6 || n == 7) ? nbm : ly;
-      }
-      const int d = S.dmap[(cy + 1) * 10 + cx + 1];
+    unsigned seen0 = 0, seen1 = 0, seen2 = 0, seen3 = 0;
+    const int n = mv_candidates(bx, by, bw, bh), off = c_slot_off[b];
+    int cnt = 0;
+    for (int k = 0; k < n; k++) {
+      const int d = S.dmap[candidate_cell(bx, by, bw, bh, k)];
       const unsigned bit = 1u << (d & 31);
-      if (seen[d >> 5] & bit) continue;  // repeated_candidate: an earlier candidate had this MV
-      seen[d >> 5] |= bit;
-      const int s = block_satd(S, b, d);
-      if (s < best) best = s, bestd = d;
+      const unsigned seen = d < 32 ? seen0 : d < 64 ? seen1 : d < 96 ? seen2 : seen3;
+      if (seen & bit) continue;  // an earlier candidate had this MV
+      if (d < 32) seen0 |= bit;
+      else if (d < 64) seen1 |= bit;
+      else if (d < 96) seen2 |= bit;
+      else seen3 |= bit;
+      S.list[off + cnt++] = (unsigned char)d;
     }
-    out[b] = make_int2(best, S.D[bestd]);
+    S.nlist[b] = (unsigned char)cnt;
+  }
+
+  // this thread's tile: cur rows in registers as 16-bit lane pairs (the grid lies inside the margin)
+  const int tx = tid & 15, ty = tid >> 4;
+  const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
+  uint32_t ce[4], co[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const uint32_t c = load4(cur.p + (long long)(oy + ty * 4 + i) * cur.stride + ox + tx * 4);
+    ce[i] = bytes_even(c), co[i] = bytes_odd(c);
+  }
+  // chunks of equal size, at most kChunk MVs each
+  const int nchunks = (nd + kChunk - 1) / kChunk, csize = (nd + nchunks - 1) / nchunks;
+  __syncthreads();  // lists complete
+
+  for (int c0 = 0; c0 < nd; c0 += csize) {
+    const int nc = min(csize, nd - c0);
+    // 2. tile SATDs at every MV of the chunk (two MVs per step for load parallelism); an 8x8
+    //    cell's tiles are lanes l, l + 1, l + 16, l + 17 of one warp
+    for (int dd = 0; dd < nc; dd += 2) {
+      int sat[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int m = S.D[c0 + min(dd + h, nc - 1)], mx = mv_x(m), my = mv_y(m);
+        DevPlane ph = ref;
+        ph.p = ref.p + (long long)((my & 3) * 4 + (mx & 3)) * ref.phase;
+        const int x = ox + tx * 4 + (mx >> 2), y = oy + ty * 4 + (my >> 2);
+        uint32_t pr[4];
+        if (inside(ph, x, y, 4, 4)) {
+          const uint8_t* p = ph.p + (long long)y * ph.stride + x;
+#pragma unroll
+          for (int i = 0; i < 4; i++) pr[i] = load4(p + (long long)i * ph.stride);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            pr[i] = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) pr[i] |= (uint32_t)at(ph, y + i, x + k) << (8 * k);
+          }
+        }
+        sat[h] = satd4_bytes(ce, co, pr);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        int v = sat[h] + __shfl_xor_sync(0xffffffffu, sat[h], 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        if (dd + h < nc) {
+          S.tile[dd + h][tid] = (unsigned short)sat[h];
+          if (lane < 16 && !(lane & 1)) S.whole8[dd + h][(tid >> 5) * 8 + (lane >> 1)] = (unsigned short)v;
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < nc * 16; e += kInterThreads) {
+      const int dd = e >> 4, i = e & 15, c = (i >> 2) * 16 + (i & 3) * 2;
+      const unsigned short* W = S.whole8[dd];
+      S.sum16[dd][i] = W[c] + W[c + 1] + W[c + 8] + W[c + 9];
+    }
+    __syncthreads();
+    // 3. every candidate slot whose MV is in this chunk
+    for (int e = tid; e < kSlots; e += kInterThreads) {
+      const unsigned bp = g_slot[e];
+      const int b = bp & 511, pos = bp >> 9;
+      if (pos >= S.nlist[b]) continue;
+      const int d = S.list[e] - c0;
+      if (d < 0 || d >= nc) continue;
+      atomicMin(&S.key[b], ((unsigned)block_satd(S, b, d) << 7) | (unsigned)pos);
+    }
+    __syncthreads();  // the next chunk overwrites the sums
+  }
+  int2* out = job.inter + ((long long)sb * kMaxRefs + r) * kBlocks;
+  for (int b = tid; b < kBlocks; b += kInterThreads) {
+    const unsigned k = S.key[b];
+    out[b] = make_int2((int)(k >> 7), S.D[S.list[c_slot_off[b] + (k & 127)]]);
   }
 }
 
@@ -237,6 +268,21 @@ void launch_inter(const FrameJob* jobs, const WorkList& w, cudaStream_t st) {
 }
 
 cudaError_t inter_attributes() {
+  short off[kBlocks];
+  unsigned short slot[kSlots];
+  int o = 0;
+  for (int b = 0; b < kBlocks; b++) {
+    int x, y, w, h;
+    sb_block_geom(b, x, y, w, h);
+    const int n = ((x + w - 1) / 8 - x / 8 + 1) * ((y + h - 1) / 8 - y / 8 + 1) + 8;
+    off[b] = (short)o;
+    for (int k = 0; k < n && o + k < kSlots; k++) slot[o + k] = (unsigned short)(b | (k << 9));
+    o += n;
+  }
+  if (o != kSlots) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemcpyToSymbol(c_slot_off, off, sizeof off);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_slot, slot, sizeof slot);
+  if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InterSmem));
 }
 

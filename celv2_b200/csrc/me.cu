@@ -74,10 +74,14 @@ __device__ __forceinline__ int satd8_q(const uint32_t* c, const DevPlane& ref, i
   for (int ty = 0; ty < 2; ty++)
 #pragma unroll
     for (int tx = 0; tx < 2; tx++) {
-      int d[16];
+      uint32_t ce[4], co[4], pr[4];
 #pragma unroll
-      for (int i = 0; i < 4; i++) residual_row(d + 4 * i, c[2 * (4 * ty + i) + tx], row4(ph, x + 4 * tx, y + 4 * ty + i));
-      total += hadamard4x4(d);
+      for (int i = 0; i < 4; i++) {
+        const uint32_t cw = c[2 * (4 * ty + i) + tx];
+        ce[i] = bytes_even(cw), co[i] = bytes_odd(cw);
+        pr[i] = row4(ph, x + 4 * tx, y + 4 * ty + i);
+      }
+      total += satd4_bytes(ce, co, pr);
     }
   return total;
 }
