@@ -10,16 +10,16 @@
 //     computes the six centre SADs;
 //  B. one thread per cell replays the reference's sequential choice of the two best distinct
 //     centres, and the searches (one or two per cell) get their 24 x 32-byte reference windows
-//     staged in shared memory with aligned 32-bit loads;
+//     staged in shared memory with aligned 8-byte loads;
 //  C. one thread per (search, dx) column slides down the window's 24 rows: each row's 8 bytes at
-//     column dx are loaded once (two funnel shifts of three words) and feed, with __vsadu4, every
+//     column dx are loaded once (two funnel shifts of three words) and feed, with vabsdiff4, every
 //     one of the 17 dy accumulators whose 8x8 block covers that row -- 24 row loads instead of
 //     17 x 8 per column. The column's best (cost << 9 | raster index) goes to a shared atomicMin,
 //     which yields the reference's first strict minimum in dy-major order;
 //  D. at level 0, the 9 positions of each refinement step are (cell, position) items computing the
 //     8x8 quarter-pel SATD from the phase planes; one thread per cell replays the centre-first
 //     strict choice.
-// Integer ALU bound: 289 x 16 __vsadu4 per searched centre.
+// Integer ALU bound: 289 x 16 byte-SIMD absolute-difference accumulates per searched centre.
 #include "kernels.h"
 
 namespace celv2cu {
@@ -27,7 +27,7 @@ namespace celv2cu {
 constexpr int kMeThreads = 256;
 constexpr int kMeCells = 32;                   // cells per CTA
 constexpr int kMeSearches = 2 * kMeCells;      // at most two centres per cell
-constexpr int kWinRows = 24, kWinWords = 8;    // a window row: 32 bytes from a 4-byte boundary
+constexpr int kWinRows = 24, kWinWords = 8;    // a window row: 32 bytes from an 8-byte boundary
 constexpr int kWinStride = kWinRows * kWinWords + 8;  // +8 words: neighbouring windows use other banks
 
 struct MeSmem {
@@ -53,13 +53,29 @@ __device__ __forceinline__ uint32_t row4(const DevPlane& s, int x, int y) {
   return v;
 }
 
+// acc + the sum of the four byte absolute differences of a and b (PTX vabsdiff4 with its add).
+__device__ __forceinline__ unsigned sad4_acc(unsigned a, unsigned b, unsigned acc) {
+  unsigned d;
+  asm("vabsdiff4.u32.u32.u32.add %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(acc));
+  return d;
+}
+
 // sad8 of a cur block (shared memory) against the reference at (x, y).
 __device__ __forceinline__ int sad8(const uint32_t* c, const DevPlane& ref, int x, int y) {
   unsigned s = 0;
+  if (inside(ref, x, y, 8, 8)) {
+    const uint8_t* p = ref.p + (long long)y * ref.stride + x;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      s = sad4_acc(c[2 * i], load4(p + (long long)i * ref.stride), s);
+      s = sad4_acc(c[2 * i + 1], load4(p + (long long)i * ref.stride + 4), s);
+    }
+    return (int)s;
+  }
 #pragma unroll
   for (int i = 0; i < 8; i++) {
-    s = __vsadu4(c[2 * i], row4(ref, x, y + i)) + s;
-    s = __vsadu4(c[2 * i + 1], row4(ref, x + 4, y + i)) + s;
+    s = sad4_acc(c[2 * i], row4(ref, x, y + i), s);
+    s = sad4_acc(c[2 * i + 1], row4(ref, x + 4, y + i), s);
   }
   return (int)s;
 }
@@ -69,6 +85,8 @@ __device__ __forceinline__ int satd8_q(const uint32_t* c, const DevPlane& ref, i
   DevPlane ph = ref;
   ph.p = ref.p + (long long)((qy & 3) * 4 + (qx & 3)) * ref.phase;
   const int x = x0 + (qx >> 2), y = y0 + (qy >> 2);
+  const bool in = inside(ph, x, y, 8, 8);
+  const uint8_t* p = ph.p + (long long)y * ph.stride + x;
   int total = 0;
 #pragma unroll
   for (int ty = 0; ty < 2; ty++)
@@ -79,7 +97,7 @@ __device__ __forceinline__ int satd8_q(const uint32_t* c, const DevPlane& ref, i
       for (int i = 0; i < 4; i++) {
         const uint32_t cw = c[2 * (4 * ty + i) + tx];
         ce[i] = bytes_even(cw), co[i] = bytes_odd(cw);
-        pr[i] = row4(ph, x + 4 * tx, y + 4 * ty + i);
+        pr[i] = in ? load4(p + (long long)(4 * ty + i) * ph.stride + 4 * tx) : row4(ph, x + 4 * tx, y + 4 * ty + i);
       }
       total += satd4_bytes(ce, co, pr);
     }
@@ -155,19 +173,26 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
       const int cxs = k ? px2 : px, cys = k ? py2 : py;
       const int wx0 = bx * 8 + cxs - kMeRange;
       S.scell[s0 + k] = c, S.sx[s0 + k] = cxs, S.sy[s0 + k] = cys;
-      S.soff[s0 + k] = wx0 - (wx0 & ~3);  // the window starts on the 4-byte boundary below wx0
+      S.soff[s0 + k] = wx0 - (wx0 & ~7);  // the window starts on the 8-byte boundary below wx0
       S.skey[s0 + k] = 0xffffffffu;
     }
   }
   __syncthreads();
   const int nsearch = S.nsearch;
-  // windows: rows y0 + cy - 8 .. + 23, 8 words from the 4-byte boundary at or below x0 + cx - 8
-  for (int e = tid; e < nsearch * kWinRows * kWinWords; e += kMeThreads) {
-    const int s = e / (kWinRows * kWinWords), rem = e - s * (kWinRows * kWinWords);
-    const int rr = rem >> 3, ww = rem & 7;
+  // windows: rows y0 + cy - 8 .. + 23, 32 bytes from the 8-byte boundary at or below x0 + cx - 8;
+  // inside the margin as 8-byte loads, else word by word with clamping
+  for (int e = tid; e < nsearch * kWinRows * 4; e += kMeThreads) {
+    const int s = e / (kWinRows * 4), rem = e - s * (kWinRows * 4);
+    const int rr = rem >> 2, qd = rem & 3;
     const int cell = cell0 + S.scell[s], by = cell / cols, bx = cell - by * cols;
-    const int wx = ((bx * 8 + S.sx[s] - kMeRange) & ~3) + 4 * ww, wy = by * 8 + S.sy[s] - kMeRange + rr;
-    S.win[s * kWinStride + rr * kWinWords + ww] = row4(ref, wx, wy);
+    const int wx = (bx * 8 + S.sx[s] - kMeRange) & ~7, wy = by * 8 + S.sy[s] - kMeRange;
+    uint32_t* dst = S.win + s * kWinStride + rr * kWinWords + 2 * qd;
+    if (inside(ref, wx, wy, 4 * kWinWords, kWinRows)) {
+      const uint2 v = __ldg(reinterpret_cast<const uint2*>(ref.p + (long long)(wy + rr) * ref.stride + wx + 8 * qd));
+      dst[0] = v.x, dst[1] = v.y;
+    } else {
+      dst[0] = row4(ref, wx + 8 * qd, wy + rr), dst[1] = row4(ref, wx + 8 * qd + 4, wy + rr);
+    }
   }
   __syncthreads();
 
@@ -191,7 +216,7 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         const int dy = rr - i;
-        if (dy >= 0 && dy <= 16) acc[dy] = __vsadu4(cw[2 * i + 1], w1) + (__vsadu4(cw[2 * i], w0) + acc[dy]);
+        if (dy >= 0 && dy <= 16) acc[dy] = sad4_acc(cw[2 * i + 1], w1, sad4_acc(cw[2 * i], w0, acc[dy]));
       }
     }
     unsigned best = 0xffffffffu;
