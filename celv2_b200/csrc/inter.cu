@@ -9,14 +9,14 @@
 // Work reuse: a block's SATD at an MV is the sum of its 4x4 tiles' SATDs at that MV (the blocks'
 // tiles all sit on the superblock's 4x4 grid), and every candidate MV of a superblock's blocks is
 // the level-0 MV of one of the 10 x 10 cells around it. So one CTA per (superblock, reference):
-//  1. gathers those 100 MVs (clamped into the field) and their distinct set D, and lists every
-//     block's candidates as distinct MVs in first-occurrence order (repeats dropped);
+//  1. gathers those 100 MVs (clamped into the field) and their distinct set D, and gives every
+//     (block, candidate) slot its MV's index in D, marking repeats of an earlier candidate's MV;
 //  2. for chunks of D: one thread per 4x4 tile (its cur samples in registers) computes the tile's
 //     SATD at every MV of the chunk -- a warp reads two contiguous image rows per load -- and the
 //     four tiles of an 8x8 cell, which sit in one warp, sum by shuffles; then the 16x16 sums;
-//  3. every (block, list position) slot of the chunk's MVs takes its SATD from those sums and a
-//     shared atomicMin of (SATD << 7 | position) keeps each block's least; position order is the
-//     candidates' order, so this is the first strict minimum of the reference's loop.
+//  3. every non-repeated slot whose MV is in the chunk takes its SATD from those sums, and a
+//     shared atomicMin of (SATD << 7 | candidate index) keeps each block's least -- the first
+//     strict minimum of the reference's loop over its candidates.
 // 256 |D| Hadamards per (superblock, reference) instead of up to 68,352 for the blocks one by one.
 // The result per (block, reference) is the winning SATD and MV; the lambda terms are added by the
 // finalize stage, which alone needs the costs.
@@ -30,7 +30,7 @@ constexpr int kChunk = 64;          // distinct MVs per pass at most
 constexpr int kSlots = 4296;        // candidates of the 425 blocks (cells covered + 8 neighbours)
 
 // Where block b's candidate list starts (blocks in index order, mv_candidates() slots each), and
-// for every slot its block and list position (b | position << 9).
+// for every slot its block and candidate index (b | k << 9).
 __constant__ short c_slot_off[kBlocks];
 __device__ unsigned short g_slot[kSlots];
 
@@ -39,9 +39,8 @@ struct InterSmem {
   int D[kNb];   // distinct MVs, first occurrence order
   int first_idx[kNb];
   unsigned char dmap[kNb];
-  unsigned char nlist[kBlocks];
-  unsigned char list[kSlots];         // per block: its candidates' distinct MVs, first occurrence order
-  unsigned key[kBlocks];              // per block: least (SATD << 7 | position) so far
+  unsigned char list[kSlots];         // per candidate slot: its MV index, 255 where it repeats one
+  unsigned key[kBlocks];              // per block: least (SATD << 7 | candidate index) so far
   unsigned short tile[kChunk][256];   // 4x4 SATDs (at most 16 x 4 x 255 = 16,320)
   unsigned short whole8[kChunk][64];  // 8x8 sums (at most 65,280)
   int sum16[kChunk][16];
@@ -166,24 +165,35 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   const int nd = S.nd;
   if (tid == 0 && job.stats) atomicAdd(job.stats + kStatInterMvs, (unsigned long long)nd);
   __syncthreads();
+  // every candidate slot's MV index (balanced over the threads) ...
+  for (int e = tid; e < kSlots; e += kInterThreads) {
+    const unsigned bp = g_slot[e];
+    const int b = bp & 511, k = bp >> 9;
+    int bx, by, bw, bh;
+    sb_block_geom(b, bx, by, bw, bh);
+    S.list[e] = S.dmap[candidate_cell(bx, by, bw, bh, k)];
+  }
+  __syncthreads();
+  // ... then per block, in candidate order, a repeat of an earlier candidate's MV is marked 255
   for (int b = tid; b < kBlocks; b += kInterThreads) {
     int bx, by, bw, bh;
     sb_block_geom(b, bx, by, bw, bh);
     unsigned seen0 = 0, seen1 = 0, seen2 = 0, seen3 = 0;
-    const int n = mv_candidates(bx, by, bw, bh), off = c_slot_off[b];
-    int cnt = 0;
+    unsigned char* L = S.list + c_slot_off[b];
+    const int n = mv_candidates(bx, by, bw, bh);
     for (int k = 0; k < n; k++) {
-      const int d = S.dmap[candidate_cell(bx, by, bw, bh, k)];
+      const int d = L[k];
       const unsigned bit = 1u << (d & 31);
       const unsigned seen = d < 32 ? seen0 : d < 64 ? seen1 : d < 96 ? seen2 : seen3;
-      if (seen & bit) continue;  // an earlier candidate had this MV
+      if (seen & bit) {
+        L[k] = 255;
+        continue;
+      }
       if (d < 32) seen0 |= bit;
       else if (d < 64) seen1 |= bit;
       else if (d < 96) seen2 |= bit;
       else seen3 |= bit;
-      S.list[off + cnt++] = (unsigned char)d;
     }
-    S.nlist[b] = (unsigned char)cnt;
   }
 
   // this thread's tile: cur rows in registers as 16-bit lane pairs (the grid lies inside the margin)
@@ -243,14 +253,13 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
       S.sum16[dd][i] = W[c] + W[c + 1] + W[c + 8] + W[c + 9];
     }
     __syncthreads();
-    // 3. every candidate slot whose MV is in this chunk
+    // 3. every (non-repeated) candidate slot whose MV is in this chunk
     for (int e = tid; e < kSlots; e += kInterThreads) {
-      const unsigned bp = g_slot[e];
-      const int b = bp & 511, pos = bp >> 9;
-      if (pos >= S.nlist[b]) continue;
-      const int d = S.list[e] - c0;
+      const int d = (int)S.list[e] - c0;  // 255 (a repeat) lies past every chunk
       if (d < 0 || d >= nc) continue;
-      atomicMin(&S.key[b], ((unsigned)block_satd(S, b, d) << 7) | (unsigned)pos);
+      const unsigned bp = g_slot[e];
+      const int b = bp & 511, k = bp >> 9;
+      atomicMin(&S.key[b], ((unsigned)block_satd(S, b, d) << 7) | (unsigned)k);
     }
     __syncthreads();  // the next chunk overwrites the sums
   }
