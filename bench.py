@@ -296,6 +296,14 @@ def stage_ops(counters, plan, steps):
     return ops
 
 
+def stage_units(plan, steps):
+    """Work units per stage over `steps` steps (the units of profiles/traffic.json)."""
+    cells, inter_refs, frames = plan_counts(plan)
+    nsb = ((W + 63) // 64) * ((H + 63) // 64)
+    return {"me_l0": cells[0] * steps, "inter": inter_refs * nsb * steps, "intra": frames * nsb * steps,
+            "finalize": frames * nsb * steps}
+
+
 def stage_bytes(plan, steps):
     """Minimum HBM bytes per stage over `steps` steps: every input read once, every output written once."""
     cells, inter_refs, frames = plan_counts(plan)
@@ -397,8 +405,11 @@ def run_cuda_arm(args):
         achieved = ops.get(dominant, 0.0) / dom_n / (dom_ms / dom_n / 1e3) / 1e9 if dom_n else 0.0
         traffic = None
         tr_path = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tr_path):
-            traffic = json.load(open(tr_path)).get(dominant)
+        if os.path.exists(tr_path) and dom_n:
+            per = json.load(open(tr_path)).get(dominant)
+            if per:  # ncu bytes per unit of the small case, scaled by this launch's units
+                units = stage_units(plan, 2).get(dominant, 0)
+                traffic = per["bytes_per_unit"] * units / dom_n
         hbm_bytes = stage_bytes(plan, 2).get(dominant, 0.0)
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         roofline = {"bound": "int32", "kernel": dominant, "achieved": achieved, "peak": int_peak, "unit": "Gop/s",

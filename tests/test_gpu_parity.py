@@ -235,3 +235,94 @@ def test_three_engines_on_threads(oracle):
     for t in ts:
         t.join()
     assert not errors and not bad, (errors, bad)
+
+
+def test_full_size_1080p_seven_refs(oracle):
+    """The bench's workload at full size: a 1080p 10-bit leaf frame against its 7 references
+    (the mini-GOP's reference lists), byte-identical records; the oracle runs on every host core."""
+    from bench import mini_gop_plan
+
+    clip = synth.hd_clip(seed=1, frames=17)
+    w, h = 1920, 1080
+    src, refs = mini_gop_plan()[-1][0]
+    with CudaEngine(w, h) as e:
+        got = e.decide_inter(clip[src].hy, [clip[r].hy for r in refs], 130).records
+    want = oracle.decide(w, h, clip[src].y, [clip[r].y for r in refs], lam.lambda_q8(130))
+    assert_same(got, want, "1080p leaf, 7 references")
+
+
+def test_batched_leaves_match_single_launches():
+    """A mini-GOP's leaves decided as one batch equal the same frames decided one at a time."""
+    from bench import mini_gop_plan
+
+    clip = synth.sinusoid_clip(640, 360, 17, 4, sinusoids=8, rects=12, affine_regions=(4, 3), noise_sigma=4.0)
+    leaves = mini_gop_plan()[-1]
+    with CudaEngine(640, 360) as e:
+        for i, f in enumerate(clip):
+            e.upload(f.hy, i)
+        e.launch_group([s for s, _ in leaves], [r for _, r in leaves], 130, to_host=True)
+        batched = [e.group_records(j) for j in range(len(leaves))]
+        for j, (s, refs) in enumerate(leaves):
+            single = e.decide_inter(clip[s].y, [clip[r].y for r in refs], 130).records
+            assert_same(batched[j], single, f"leaf {s}")
+
+
+def leaves_of(rec, sb_cols, sb_rows):
+    out = []
+    for sr in range(sb_rows):
+        for sc in range(sb_cols):
+            r = rec[sr * sb_cols + sc]
+            tree = list(r["tree"][: int(r["ntree"])])
+            pos, blocks = [0], []
+
+            def walk(x, y, bw, bh):
+                p = tree[pos[0]]
+                pos[0] += 1
+                if p == 0:
+                    blocks.append((x, y, bw, bh))
+                elif p == 1:
+                    walk(x, y, bw, bh // 2), walk(x, y + bh // 2, bw, bh // 2)
+                elif p == 2:
+                    walk(x, y, bw // 2, bh), walk(x + bw // 2, y, bw // 2, bh)
+                else:
+                    for q in range(4):
+                        walk(x + (q & 1) * bw // 2, y + (q >> 1) * bh // 2, bw // 2, bh // 2)
+
+            walk(sc * 64, sr * 64, 64, 64)
+            out += [(*b, r, k) for k, b in enumerate(blocks)]
+    return out
+
+
+def test_cuda_finds_integer_and_quarter_pel_motion():
+    """Known answers of tests/test_gpu_me.cpp:71-163 on the CUDA engine: (5, -3) px on >= 90% of
+    the interior, (2.5, -1.25) px on >= 75% of the inter area."""
+    w, h = 640, 360
+    with CudaEngine(w, h) as e:
+        rec = e.decide_inter(F.textured(w, h, 5, -3), [F.textured(w, h, 0, 0)], 120).records
+    interior = hit = 0
+    for x, y, bw, bh, r, k in leaves_of(rec, 10, 6):
+        if x < 16 or y < 16 or x + bw > w - 16 or y + bh > h - 16:
+            continue
+        interior += bw * bh
+        hit += bw * bh if (r["mode"][k] == 13 and r["mvx"][k] == 20 and r["mvy"][k] == -12) else 0
+    assert interior > 0 and hit * 10 >= interior * 9
+    w, h = 320, 192
+    with CudaEngine(w, h) as e:
+        rec = e.decide_inter(F.smooth(w, h, 2.5, -1.25), [F.smooth(w, h, 0, 0)], 60).records
+    inter = hit = 0
+    for r in rec:
+        for k in range(int(r["nblocks"])):
+            if r["mode"][k] == 13:
+                a = int(r["w4"][k]) * int(r["h4"][k])
+                inter += a
+                hit += a if (r["mvx"][k], r["mvy"][k]) == (10, -5) else 0
+    assert inter > 0 and hit * 4 >= inter * 3
+
+
+def test_cuda_finds_large_motion():
+    """tests/test_gpu_me.cpp:293-308 on the CUDA engine's level-0 field: (96, 24) px."""
+    with CudaEngine(640, 360) as e:
+        e.decide_inter(F.scene_frame(640, 360, 96, 24), [F.scene_frame(640, 360, 0, 0)], 120)
+        fx, fy = unpack_field(e.debug_field(0, 0))
+    sub = (fx[4:, 13:] == -96 * 4) & (fy[4:, 13:] == -24 * 4)
+    assert sub.sum() * 4 >= sub.size * 3
