@@ -335,6 +335,12 @@ def run_cuda_arm(args):
     for i, f in enumerate(clip):
         eng.upload(f.hy, i)  # 10-bit planes; the device rounds them to the 8-bit samples it scores
     stream = torch.cuda.ExternalStream(eng.stream(), device=f"cuda:{local}")
+    # launch configuration per frame size (decisions do not depend on it), before any timing
+    from celv2_b200 import tune
+
+    leaf_src, leaf_refs = plan[-1][0]
+    tuned = tune.autotune(eng, leaf_src, leaf_refs, QINDEX) if not args.no_tune else None
+    eng.set_config(E.CFG_GRAPHS, 0 if args.no_graphs else 1)
 
     def step():
         for group in plan:
@@ -435,7 +441,9 @@ def run_cuda_arm(args):
                 "config": {"workload": "1080p10 mini-GOP: 17 frames 1920x1080, hidden anchor + pyramid, refs 7, "
                                        "qindex 130; leaves batched", "frames_per_step": NFRAMES, "refs": REFS,
                            "qindex": QINDEX, "parallelism": f"replicas x{world}",
-                           "l2": "inputs larger than L2 (17 resident frames with phase planes, ~1.2 GB per rank)"},
+                           "l2": "inputs larger than L2 (17 resident frames with phase planes, ~1.2 GB per rank)",
+                           "launch": {"persistent_queue_kernels": True, "cuda_graphs": not args.no_graphs,
+                                      "tuned": {k: v for k, v in (tuned or {}).items() if k != "stage_ms"}}},
                 "clocks": clocks.summary(), "gpu_launches": launches,
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps, "api": "launch/prepare/collect per frame (celv2_launch, celv2_wait_row)"},
@@ -471,6 +479,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default launch configuration")
+    ap.add_argument("--no-graphs", action="store_true", help="stage-by-stage launches instead of CUDA graphs")
     ap.add_argument("--profile", action="store_true", help="the small case for ncu captures")
     args = ap.parse_args()
     if args.profile:

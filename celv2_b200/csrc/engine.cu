@@ -42,10 +42,32 @@ using namespace celv2cu;
 
 namespace {
 thread_local std::string g_error;
+std::mutex g_grid_mu;
+struct GridKey {
+  const void* kernel;
+  int device, threads;
+  size_t smem;
+};
+std::vector<std::pair<GridKey, int>> g_grid_cache;  // CTAs per SM x SMs, per kernel and device
 }  // namespace
 
 // The calling thread's message for celv2_last_error (entry points outside this file set it too).
 void celv2cu::set_last_error(const std::string& msg) { g_error = msg; }
+
+int celv2cu::persistent_grid(const void* kernel, int threads, size_t smem, int units) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_grid_mu);
+  for (const auto& e : g_grid_cache)
+    if (e.first.kernel == kernel && e.first.device == dev && e.first.threads == threads && e.first.smem == smem)
+      return units < e.second ? units : e.second;
+  int per_sm = 1, sms = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int full = (per_sm < 1 ? 1 : per_sm) * sms;
+  g_grid_cache.push_back({GridKey{kernel, dev, threads, smem}, full});
+  return units < full ? units : full;
+}
 
 namespace {
 
@@ -201,6 +223,13 @@ struct celv2_engine {
   double stage_ms[kStages] = {};
   long long stage_n[kStages] = {};
   unsigned long long* stats = nullptr;  // device work counters (kStats), while timing
+  // stage work queues (device counters): [0..4] motion search levels, [5] intra, [6] inter,
+  // [7] finalize of the main stream; [8] prepare's intra
+  unsigned* queues = nullptr;
+  bool persistent = true;      // the queue-draining persistent stage kernels (else one CTA per unit)
+  unsigned persistent_off = 0; // stages (bit i: queue i) that run one CTA per unit anyway
+  int me_cells[kLevels] = {32, 32, 32, 32, 32};
+  int inter_chunk = 64;
 
   template <typename F>
   void stage(int id, cudaStream_t stream, F&& f) {
@@ -239,6 +268,7 @@ struct celv2_engine {
     cudaSetDevice(device);
     if (st) cudaStreamSynchronize(st);
     if (prep_st) cudaStreamSynchronize(prep_st);
+    free_graphs();
     for (Slot* s : store) cudaFree(s->mem), delete s;
     for (Slot& s : srcs) cudaFree(s.mem);
     for (Stage& s : stages) {
@@ -253,6 +283,7 @@ struct celv2_engine {
     for (cudaEvent_t e : row_done) cudaEventDestroy(e);
     for (const Timed& t : timed) cudaEventDestroy(t.a), cudaEventDestroy(t.b);
     cudaFree(stats);
+    cudaFree(queues);
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     cudaFree(djobs);
     cudaFreeHost(ring);
@@ -284,6 +315,7 @@ struct celv2_engine {
     CK(cudaStreamCreateWithFlags(&prep_st, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&prep_done, cudaEventDisableTiming));
     CK(cudaMalloc(&djobs, kRingJobs * sizeof(FrameJob)));
+    CK(cudaMalloc(&queues, 16 * sizeof(unsigned)));
     CK(cudaMallocHost(&ring, (size_t)kRing * kRingJobs * sizeof(FrameJob)));
     for (cudaEvent_t& e : ring_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     alloc_buffers(single, false);
@@ -435,46 +467,48 @@ struct celv2_engine {
     ring_pending[i] = true;
   }
 
-  // The stage kernels of the jobs; intra for the jobs flagged.
-  void run_stages(const std::vector<FrameJob>& jobs, const std::vector<char>& need_intra, cudaStream_t stream) {
+  // Queues the stage kernels of the jobs whose descriptors are in djobs (intra for all of them
+  // or none); returns the kernels launched.
+  int enqueue_stages(const std::vector<FrameJob>& jobs, bool with_intra, cudaStream_t stream) {
     const int n = (int)jobs.size();
-    put_jobs(jobs.data(), n, djobs, stream);
+    int launched = 0;
+    if (persistent) CK(cudaMemsetAsync(queues, 0, 8 * sizeof(unsigned), stream));
+    auto q = [&](int i) { return persistent && !(persistent_off >> i & 1) ? queues + i : nullptr; };
     WorkList w{};
     w.njobs = n;
     for (int l = kLevels - 1; l >= 0; l--) {
-      for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + me_units(jobs[j].nrefs, jobs[j].fcols[l], jobs[j].frows[l]);
+      for (int j = 0; j < n; j++)
+        w.prefix[j + 1] = w.prefix[j] + me_units(jobs[j].nrefs, jobs[j].fcols[l], jobs[j].frows[l], me_cells[l]);
+      w.queue = q(l);
       if (w.prefix[n] > 0) {
-        stage(kStMe0 - l, stream, [&] { launch_me_level(djobs, w, l, stream); });
-        kernel_launches++;
+        stage(kStMe0 - l, stream, [&] { launch_me_level(djobs, w, l, me_cells[l], stream); });
+        launched++;
       }
     }
-    for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + (need_intra[j] ? jobs[j].sb_cols * jobs[j].sb_rows : 0);
-    if (w.prefix[n] > 0) {
-      // only the flagged jobs: a list of them with their own prefix
-      std::vector<FrameJob> sub;
-      for (int j = 0; j < n; j++)
-        if (need_intra[j]) sub.push_back(jobs[j]);
-      if ((int)sub.size() == n) {
-        stage(kStIntra, stream, [&] { launch_intra(djobs, w, stream); });
-      } else {
-        // the flagged jobs' descriptors go after the batch's
-        put_jobs(sub.data(), (int)sub.size(), djobs + n, stream);
-        WorkList ws{};
-        ws.njobs = (int)sub.size();
-        for (int j = 0; j < ws.njobs; j++) ws.prefix[j + 1] = ws.prefix[j] + sub[j].sb_cols * sub[j].sb_rows;
-        stage(kStIntra, stream, [&] { launch_intra(djobs + n, ws, stream); });
-      }
-      kernel_launches++;
+    if (with_intra) {
+      for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].sb_cols * jobs[j].sb_rows;
+      w.queue = q(5);
+      stage(kStIntra, stream, [&] { launch_intra(djobs, w, stream); });
+      launched++;
     }
     for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].nrefs * jobs[j].sb_cols * jobs[j].sb_rows;
+    w.queue = q(6);
     if (w.prefix[n] > 0) {
-      stage(kStInter, stream, [&] { launch_inter(djobs, w, stream); });
-      kernel_launches++;
+      stage(kStInter, stream, [&] { launch_inter(djobs, w, inter_chunk, stream); });
+      launched++;
     }
     for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].sb_cols * jobs[j].sb_rows;
+    w.queue = q(7);
     stage(kStFinalize, stream, [&] { launch_finalize(djobs, w, stream); });
-    kernel_launches++;
+    launched++;
     CK(cudaGetLastError());
+    return launched;
+  }
+
+  // The stage kernels of the jobs, their descriptors sent through the pinned ring.
+  void run_stages(const std::vector<FrameJob>& jobs, bool with_intra, cudaStream_t stream) {
+    put_jobs(jobs.data(), (int)jobs.size(), djobs, stream);
+    kernel_launches += enqueue_stages(jobs, with_intra, stream);
   }
 
   void wait_idle() {
@@ -524,7 +558,7 @@ struct celv2_engine {
       }
       std::vector<FrameJob> jobs(1);
       fill_job(jobs[0], srcs[use].pyr, used, nrefs, single, intra_prep[use], lam);
-      run_stages(jobs, std::vector<char>{static_cast<char>(!prepared)}, st);
+      run_stages(jobs, !prepared, st);
       last_nrefs = nrefs;
       // rows back to the host in row-stream order
       const int streams = std::max(1, std::min(row_streams, g.sb_rows));
@@ -564,6 +598,10 @@ struct celv2_engine {
     WorkList w{};
     w.njobs = 1;
     w.prefix[1] = g.nsb;
+    if (persistent) {
+      CK(cudaMemsetAsync(queues + 8, 0, sizeof(unsigned), prep_st));
+      w.queue = queues + 8;
+    }
     stage(kStIntra, prep_st, [&] { launch_intra(dprep, w, prep_st); });
     kernel_launches++;
     CK(cudaGetLastError());
@@ -582,6 +620,7 @@ struct celv2_engine {
   void reserve_group(int frames) {
     if (frames <= group_cap) return;
     wait_idle();
+    free_graphs();  // they hold the old buffers' addresses
     for (JobBuffers& b : group) free_buffers(b);
     group.assign(frames, JobBuffers{});
     for (JobBuffers& b : group) alloc_buffers(b, true);
@@ -629,20 +668,175 @@ struct celv2_engine {
       }
       fill_job(jobs[j], cur->pyr, refs, nrefs[j], group[j], group[j].intra, lams[j]);
     }
-    run_stages(jobs, std::vector<char>(njobs, 1), st);
-    if (to_host)
-      for (int j = 0; j < njobs; j++)
-        CK(cudaMemcpyAsync(group_host + (size_t)j * g.nsb, group[j].out, g.nsb * sizeof(celv2_sb_out),
-                           cudaMemcpyDeviceToHost, st));
+    if (use_graphs && !timing) {
+      launch_graph(jobs, to_host);
+    } else {
+      run_stages(jobs, true, st);
+      if (to_host)
+        for (int j = 0; j < njobs; j++)
+          CK(cudaMemcpyAsync(group_host + (size_t)j * g.nsb, group[j].out, g.nsb * sizeof(celv2_sb_out),
+                             cudaMemcpyDeviceToHost, st));
+    }
     group_jobs = njobs;
     ++launches;
     pending = true;
   }
+
+  // ---- CUDA graphs: a batch's whole stage sequence captured once per shape, then replayed ----
+  struct Graph {
+    std::vector<int> key;  // to_host, then each job's reference count
+    cudaGraphExec_t exec = nullptr;
+    FrameJob* host_jobs = nullptr;  // pinned: the replay's descriptor copy reads it
+    cudaEvent_t done = nullptr;
+    bool replayed = false;
+    int kernels = 0;
+  };
+  bool use_graphs = false;
+  std::vector<Graph> graphs;
+
+  void free_graphs() {
+    for (Graph& gr : graphs) {
+      if (gr.exec) cudaGraphExecDestroy(gr.exec);
+      if (gr.host_jobs) cudaFreeHost(gr.host_jobs);
+      if (gr.done) cudaEventDestroy(gr.done);
+    }
+    graphs.clear();
+  }
+
+  void launch_graph(const std::vector<FrameJob>& jobs, bool to_host) {
+    std::vector<int> key{to_host ? 1 : 0};
+    for (const FrameJob& j : jobs) key.push_back(j.nrefs);
+    Graph* gr = nullptr;
+    for (Graph& x : graphs)
+      if (x.key == key) gr = &x;
+    const int n = (int)jobs.size();
+    if (!gr) {
+      graphs.emplace_back();
+      gr = &graphs.back();
+      gr->key = key;
+      CK(cudaMallocHost(&gr->host_jobs, kMaxJobs * sizeof(FrameJob)));
+      CK(cudaEventCreateWithFlags(&gr->done, cudaEventDisableTiming));
+      cudaGraph_t graph = nullptr;
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        CK(cudaMemcpyAsync(djobs, gr->host_jobs, n * sizeof(FrameJob), cudaMemcpyHostToDevice, st));
+        gr->kernels = enqueue_stages(jobs, true, st);
+        if (to_host)
+          for (int j = 0; j < n; j++)
+            CK(cudaMemcpyAsync(group_host + (size_t)j * g.nsb, group[j].out, g.nsb * sizeof(celv2_sb_out),
+                               cudaMemcpyDeviceToHost, st));
+      } catch (...) {
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        graphs.pop_back();
+        throw;
+      }
+      CK(cudaStreamEndCapture(st, &graph));
+      const cudaError_t e = cudaGraphInstantiate(&gr->exec, graph, 0);
+      cudaGraphDestroy(graph);
+      CK(e);
+    }
+    if (gr->replayed) CK(cudaEventSynchronize(gr->done));  // the last replay has read host_jobs
+    std::memcpy(gr->host_jobs, jobs.data(), n * sizeof(FrameJob));
+    CK(cudaGraphLaunch(gr->exec, st));
+    CK(cudaEventRecord(gr->done, st));
+    gr->replayed = true;
+    kernel_launches += gr->kernels;
+  }
 };
+
+namespace {
+
+// Jobs of several engines (each its own resolution and frame store) in one launch per stage, on
+// the first engine's stream. Engine e's jobs take its group slots in order of appearance.
+void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_keys, const int* nrefs,
+                  const long long* const* ref_keys, const int64_t* lams, bool to_host) {
+  if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per batch");
+  celv2_engine* lead = engines[0];
+  std::vector<celv2_engine*> uniq;
+  for (int j = 0; j < njobs; j++) {
+    if (!engines[j]) invalid("null engine");
+    if (engines[j]->device != lead->device) invalid("a batch runs on one GPU");
+    if (std::find(uniq.begin(), uniq.end(), engines[j]) == uniq.end()) uniq.push_back(engines[j]);
+  }
+  for (celv2_engine* e : uniq) {
+    int count = 0;
+    for (int j = 0; j < njobs; j++) count += engines[j] == e;
+    if (count > e->group_cap) e->reserve_group(std::max(count, 8));
+  }
+  // the stores' uploads first: the lead stream waits for every other engine's stream
+  for (celv2_engine* e : uniq)
+    if (e != lead) {
+      cudaEvent_t ev;
+      CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+      CK(cudaEventRecord(ev, e->st));
+      CK(cudaStreamWaitEvent(lead->st, ev, 0));
+      cudaEventDestroy(ev);
+    }
+  struct Entry {
+    FrameJob job;
+    celv2_engine* e;
+    int slot;
+    long long work;
+  };
+  std::vector<Entry> entries;
+  std::vector<int> next(uniq.size(), 0);
+  for (int j = 0; j < njobs; j++) {
+    celv2_engine* e = engines[j];
+    const int ei = (int)(std::find(uniq.begin(), uniq.end(), e) - uniq.begin());
+    const int slot = next[ei]++;
+    Slot* cur = e->find(src_keys[j]);
+    if (!cur) invalid("batch: no stored frame with the source key");
+    if (nrefs[j] < 0 || nrefs[j] > kMaxRefs) invalid("batch: too many references");
+    if (nrefs[j] > 0 && (e->g.pw < 16 || e->g.ph < 16)) invalid("batch: inter frames need at least 9x9 pixels");
+    Slot* refs[kMaxRefs];
+    for (int r = 0; r < nrefs[j]; r++) {
+      refs[r] = e->find(ref_keys[j][r]);
+      if (!refs[r]) invalid("batch: no stored frame with a reference key");
+      e->make_phases(*refs[r], lead->st);
+    }
+    Entry en;
+    e->fill_job(en.job, cur->pyr, refs, nrefs[j], e->group[slot], e->group[slot].intra, lams[j]);
+    en.e = e, en.slot = slot, en.work = (long long)(nrefs[j] + 1) * e->g.nsb;
+    entries.push_back(en);
+  }
+  // the largest jobs first, so the queues' last units are small ones
+  std::stable_sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) { return a.work > b.work; });
+  std::vector<FrameJob> jobs;
+  for (const Entry& en : entries) jobs.push_back(en.job);
+  lead->run_stages(jobs, true, lead->st);
+  if (to_host)
+    for (const Entry& en : entries)
+      CK(cudaMemcpyAsync(en.e->group_host + (size_t)en.slot * en.e->g.nsb, en.e->group[en.slot].out,
+                         en.e->g.nsb * sizeof(celv2_sb_out), cudaMemcpyDeviceToHost, lead->st));
+  // every engine's later work waits for this batch
+  cudaEvent_t done;
+  CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+  CK(cudaEventRecord(done, lead->st));
+  for (size_t i = 0; i < uniq.size(); i++) {
+    celv2_engine* e = uniq[i];
+    if (e != lead) CK(cudaStreamWaitEvent(e->st, done, 0));
+    e->group_jobs = next[i];
+    ++e->launches;
+    e->pending = true;
+  }
+  cudaEventDestroy(done);
+}
+
+}  // namespace
 
 extern "C" {
 
 const char* celv2_last_error(void) { return g_error.c_str(); }
+
+int celv2_launch_multi(int njobs, celv2_engine* const* engines, const long long* src_keys, const int* nrefs,
+                       const long long* const* ref_keys, const int64_t* lambda_q8, int to_host) {
+  return guarded([&] {
+    if (!engines || !src_keys || !nrefs || !lambda_q8 || njobs <= 0 || !engines[0]) invalid("null argument");
+    CK(cudaSetDevice(engines[0]->device));
+    launch_multi(njobs, engines, src_keys, nrefs, ref_keys, lambda_q8, to_host != 0);
+  });
+}
 
 int celv2_create(int width, int height, int sb_size, int device, celv2_engine** out) {
   if (out) *out = nullptr;
@@ -805,6 +999,50 @@ int celv2_debug_inter(celv2_engine* e, int32_t* out) {
 }
 
 long long celv2_kernel_launches(const celv2_engine* e) { return e ? e->kernel_launches : 0; }
+
+int celv2_set_config(celv2_engine* e, int key, int value) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    switch (key) {
+      case CELV2_CFG_PERSISTENT: e->persistent = value != 0, e->free_graphs(); break;
+      case CELV2_CFG_GRAPHS: e->use_graphs = value != 0; break;
+      case CELV2_CFG_PERSISTENT_OFF: e->persistent_off = (unsigned)value & 0xff, e->free_graphs(); break;
+      case CELV2_CFG_INTER_CHUNK:
+        if (value < 8 || value > 64) invalid("inter chunk must be 8..64");
+        e->inter_chunk = value, e->free_graphs();
+        break;
+      case CELV2_CFG_ME_CELLS_L0:
+      case CELV2_CFG_ME_CELLS_L0 + 1:
+      case CELV2_CFG_ME_CELLS_L0 + 2:
+      case CELV2_CFG_ME_CELLS_L0 + 3:
+      case CELV2_CFG_ME_CELLS_L0 + 4:
+        if (value != 16 && value != 32) invalid("motion-search cells per CTA must be 16 or 32");
+        e->me_cells[key - CELV2_CFG_ME_CELLS_L0] = value, e->free_graphs();
+        break;
+      default: invalid("unknown configuration key");
+    }
+  });
+}
+
+int celv2_get_config(const celv2_engine* e, int key, int* value) {
+  return guarded([&] {
+    if (!e || !value) invalid("null argument");
+    switch (key) {
+      case CELV2_CFG_PERSISTENT: *value = e->persistent; break;
+      case CELV2_CFG_GRAPHS: *value = e->use_graphs; break;
+      case CELV2_CFG_PERSISTENT_OFF: *value = (int)e->persistent_off; break;
+      case CELV2_CFG_INTER_CHUNK: *value = e->inter_chunk; break;
+      case CELV2_CFG_ME_CELLS_L0:
+      case CELV2_CFG_ME_CELLS_L0 + 1:
+      case CELV2_CFG_ME_CELLS_L0 + 2:
+      case CELV2_CFG_ME_CELLS_L0 + 3:
+      case CELV2_CFG_ME_CELLS_L0 + 4: *value = e->me_cells[key - CELV2_CFG_ME_CELLS_L0]; break;
+      default: invalid("unknown configuration key");
+    }
+  });
+}
 
 int celv2_stream(const celv2_engine* e, void** stream) {
   return guarded([&] {

@@ -37,11 +37,13 @@ struct FinSmem {
   int ntree, nblocks;
 };
 
-__global__ void __launch_bounds__(kFinThreads) k_finalize(const FrameJob* __restrict__ jobs, WorkList w) {
+__global__ void __launch_bounds__(kFinThreads, 3) k_finalize(const FrameJob* __restrict__ jobs, WorkList w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FinSmem& S = *reinterpret_cast<FinSmem*>(smem_raw);
+  __shared__ int unit_slot;
   const int tid = threadIdx.x;
-  const int unit = blockIdx.x;
+  int unit, iter = 0;
+  while (take_unit(w, unit, iter, &unit_slot)) {
   const int jb = job_of(w, unit);
   const FrameJob& job = jobs[jb];
   const int sb = unit - w.prefix[jb], sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
@@ -243,16 +245,20 @@ __global__ void __launch_bounds__(kFinThreads) k_finalize(const FrameJob* __rest
       o->mv2x[k] = o->mv2y[k] = 0;
     }
   }
+  }  // units
 }
 
 void launch_finalize(const FrameJob* jobs, const WorkList& w, cudaStream_t st) {
   const int units = w.prefix[w.njobs];
   if (units <= 0) return;
-  k_finalize<<<units, kFinThreads, sizeof(FinSmem), st>>>(jobs, w);
+  const int grid = w.queue ? persistent_grid((const void*)k_finalize, kFinThreads, sizeof(FinSmem), units) : units;
+  k_finalize<<<grid, kFinThreads, sizeof(FinSmem), st>>>(jobs, w);
 }
 
 cudaError_t finalize_attributes() {
-  return cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FinSmem));
+  const cudaError_t e = cudaFuncSetAttribute(k_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(FinSmem));
+  if (e == cudaSuccess) persistent_grid((const void*)k_finalize, kFinThreads, sizeof(FinSmem), 1);  // fills the grid cache
+  return e;
 }
 
 }  // namespace celv2cu

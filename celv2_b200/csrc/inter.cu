@@ -121,12 +121,14 @@ __device__ __forceinline__ int mv_candidates(int bx, int by, int bw, int bh) {
   return (((bx + bw - 1) >> 3) - (bx >> 3) + 1) * (((by + bh - 1) >> 3) - (by >> 3) + 1) + 8;
 }
 
-__global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __restrict__ jobs, WorkList w) {
+__global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __restrict__ jobs, WorkList w, int chunk) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   InterSmem& S = *reinterpret_cast<InterSmem*>(smem_raw);
   __shared__ int warp_cnt[kInterThreads / 32];
+  __shared__ int unit_slot;
   const int tid = threadIdx.x, lane = tid & 31;
-  const int unit = blockIdx.x;
+  int unit, iter = 0;
+  while (take_unit(w, unit, iter, &unit_slot)) {
   const int jb = job_of(w, unit);
   const FrameJob& job = jobs[jb];
   const int nsb = job.sb_cols * job.sb_rows;
@@ -205,8 +207,8 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
     const uint32_t c = load4(cur.p + (long long)(oy + ty * 4 + i) * cur.stride + ox + tx * 4);
     ce[i] = bytes_even(c), co[i] = bytes_odd(c);
   }
-  // chunks of equal size, at most kChunk MVs each
-  const int nchunks = (nd + kChunk - 1) / kChunk, csize = (nd + nchunks - 1) / nchunks;
+  // chunks of equal size, at most `chunk` MVs each
+  const int nchunks = (nd + chunk - 1) / chunk, csize = (nd + nchunks - 1) / nchunks;
   __syncthreads();  // lists complete
 
   for (int c0 = 0; c0 < nd; c0 += csize) {
@@ -268,12 +270,15 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
     const unsigned k = S.key[b];
     out[b] = make_int2((int)(k >> 7), S.D[S.list[c_slot_off[b] + (k & 127)]]);
   }
+  }  // units
 }
 
-void launch_inter(const FrameJob* jobs, const WorkList& w, cudaStream_t st) {
+void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, cudaStream_t st) {
   const int units = w.prefix[w.njobs];
   if (units <= 0) return;
-  k_inter<<<units, kInterThreads, sizeof(InterSmem), st>>>(jobs, w);
+  chunk = chunk < 8 ? 8 : chunk > kChunk ? kChunk : chunk;
+  const int grid = w.queue ? persistent_grid((const void*)k_inter, kInterThreads, sizeof(InterSmem), units) : units;
+  k_inter<<<grid, kInterThreads, sizeof(InterSmem), st>>>(jobs, w, chunk);
 }
 
 cudaError_t inter_attributes() {
@@ -292,7 +297,9 @@ cudaError_t inter_attributes() {
   cudaError_t e = cudaMemcpyToSymbol(c_slot_off, off, sizeof off);
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_slot, slot, sizeof slot);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InterSmem));
+  e = cudaFuncSetAttribute(k_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InterSmem));
+  if (e == cudaSuccess) persistent_grid((const void*)k_inter, kInterThreads, sizeof(InterSmem), 1);  // fills the grid cache
+  return e;
 }
 
 }  // namespace celv2cu

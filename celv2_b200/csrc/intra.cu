@@ -54,8 +54,10 @@ __device__ __forceinline__ int exact_div(int n, int d, float rcp) {
 __global__ void __launch_bounds__(kIntraThreads, 3) k_intra(const FrameJob* __restrict__ jobs, WorkList w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   IntraSmem& S = *reinterpret_cast<IntraSmem*>(smem_raw);
+  __shared__ int unit_slot;
   const int tid = threadIdx.x;
-  const int unit = blockIdx.x;
+  int unit, iter = 0;
+  while (take_unit(w, unit, iter, &unit_slot)) {
   const int jb = job_of(w, unit);
   const FrameJob& job = jobs[jb];
   const int sb = unit - w.prefix[jb], sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
@@ -231,16 +233,20 @@ __global__ void __launch_bounds__(kIntraThreads, 3) k_intra(const FrameJob* __re
   __syncthreads();
   int* out = const_cast<int*>(job.intra) + (long long)sb * kBlocks * kModes;
   for (int e = tid; e < kBlocks * kModes; e += kIntraThreads) out[e] = (&S.acc[0][0])[e];
+  }  // units
 }
 
 void launch_intra(const FrameJob* jobs, const WorkList& w, cudaStream_t st) {
   const int units = w.prefix[w.njobs];
   if (units <= 0) return;
-  k_intra<<<units, kIntraThreads, sizeof(IntraSmem), st>>>(jobs, w);
+  const int grid = w.queue ? persistent_grid((const void*)k_intra, kIntraThreads, sizeof(IntraSmem), units) : units;
+  k_intra<<<grid, kIntraThreads, sizeof(IntraSmem), st>>>(jobs, w);
 }
 
 cudaError_t intra_attributes() {
-  return cudaFuncSetAttribute(k_intra, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(IntraSmem));
+  const cudaError_t e = cudaFuncSetAttribute(k_intra, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(IntraSmem));
+  if (e == cudaSuccess) persistent_grid((const void*)k_intra, kIntraThreads, sizeof(IntraSmem), 1);  // fills the grid cache
+  return e;
 }
 
 }  // namespace celv2cu

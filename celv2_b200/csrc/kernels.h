@@ -13,10 +13,33 @@ namespace celv2cu {
 constexpr int kMaxJobs = 32;
 
 // Units of one stage per job, as prefix sums: job j owns units [prefix[j], prefix[j + 1]).
+// queue: the stage's work queue in device memory (zero before the launch) -- a persistent grid's
+// CTAs take units from it in order until it runs dry; null: one CTA per unit (blockIdx.x).
 struct WorkList {
   int njobs;
   int prefix[kMaxJobs + 1];
+  unsigned* queue;
 };
+
+// The next unit of this CTA into `unit` (every thread gets it); false when the stage is done.
+// Starts with a barrier, so the previous unit's shared state is free for the next one. No CTA
+// ever waits for another: a drained queue simply ends the loop.
+__device__ __forceinline__ bool take_unit(const WorkList& w, int& unit, int& iter, int* slot) {
+  const int total = w.prefix[w.njobs];
+  if (!w.queue) {
+    if (iter++) return false;
+    unit = blockIdx.x;
+    return unit < total;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *slot = (int)atomicAdd(w.queue, 1u);
+  __syncthreads();
+  unit = *slot;
+  return unit < total;
+}
+
+// CTAs of a persistent grid for a kernel: the SM count times the CTAs an SM holds, at most units.
+int persistent_grid(const void* kernel, int threads, size_t smem, int units);
 
 // Unit u's job (a linear scan: at most kMaxJobs jobs).
 __device__ __forceinline__ int job_of(const WorkList& w, int u) {
@@ -31,16 +54,17 @@ void launch_pyramid(const DevPyramid& pyr, cudaStream_t st);
 void launch_phases(const DevPlane& lv0, cudaStream_t st);
 
 // Motion search of one pyramid level for every (job, reference, 8x8 cell); level 0 includes the
-// quarter-pel refinement. Units: me_units(nrefs, fcols[level], frows[level]) per job (groups of
-// 32 cells of one reference).
-int me_units(int nrefs, int cols, int rows);
-void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, cudaStream_t st);
+// quarter-pel refinement. Units: me_units(nrefs, fcols[level], frows[level], cells) per job (groups
+// of `cells` cells of one reference; cells 16 or 32).
+int me_units(int nrefs, int cols, int rows, int cells);
+void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, int cells, cudaStream_t st);
 
 // Intra SATDs of every candidate block and mode. Units: sb_cols * sb_rows per job.
 void launch_intra(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
 
-// Each reference's best candidate MV per candidate block. Units: nrefs * sb_cols * sb_rows per job.
-void launch_inter(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
+// Each reference's best candidate MV per candidate block, the distinct MVs of a superblock taken
+// in chunks of at most `chunk` (<= 64). Units: nrefs * sb_cols * sb_rows per job.
+void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, cudaStream_t st);
 
 // Per-block choice, compound, partition choice and the decision records. Units: superblocks.
 void launch_finalize(const FrameJob* jobs, const WorkList& w, cudaStream_t st);

@@ -25,22 +25,24 @@
 namespace celv2cu {
 
 constexpr int kMeThreads = 256;
-constexpr int kMeCells = 32;                   // cells per CTA
-constexpr int kMeSearches = 2 * kMeCells;      // at most two centres per cell
 constexpr int kWinRows = 24, kWinWords = 8;    // a window row: 32 bytes from an 8-byte boundary
 constexpr int kWinStride = kWinRows * kWinWords + 8;  // +8 words: neighbouring windows use other banks
 
+// Shared state of a CTA of CELLS cells (16 or 32: fewer cells per CTA give small pyramid levels
+// more CTAs; the autotuner picks per level).
+template <int CELLS>
 struct MeSmem {
-  uint32_t cur[kMeCells][16];
-  int csad[kMeCells][6];
-  int ccx[kMeCells][6], ccy[kMeCells][6];
-  int scell[kMeSearches], sx[kMeSearches], sy[kMeSearches], soff[kMeSearches];
-  unsigned skey[kMeSearches];
-  int first_search[kMeCells], two[kMeCells];
-  int mvx[kMeCells], mvy[kMeCells];
-  int rsatd[kMeCells][9];
+  static constexpr int kSearches = 2 * CELLS;  // at most two centres per cell
+  uint32_t cur[CELLS][16];
+  int csad[CELLS][6];
+  int ccx[CELLS][6], ccy[CELLS][6];
+  int scell[kSearches], sx[kSearches], sy[kSearches], soff[kSearches];
+  unsigned skey[kSearches];
+  int first_search[CELLS], two[CELLS];
+  int mvx[CELLS], mvy[CELLS];
+  int rsatd[CELLS][9];
   int nsearch;
-  uint32_t win[kMeSearches * kWinStride];
+  uint32_t win[kSearches * kWinStride];
 };
 
 // 4 bytes of a plane at (x .. x + 3, y), clamped like Plane::at where the row leaves the margin.
@@ -107,11 +109,15 @@ __device__ __forceinline__ int satd8_q(const uint32_t* c, const DevPlane& ref, i
 // The refinement step's position n (raster 0..8 with the centre, 4, visited first).
 __device__ __forceinline__ int refine_pos(int t) { return t == 0 ? 4 : (t <= 4 ? t - 1 : t); }
 
+template <int CELLS>
 __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restrict__ jobs, WorkList w, int level) {
+  constexpr int kMeCells = CELLS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  MeSmem& S = *reinterpret_cast<MeSmem*>(smem_raw);
+  MeSmem<CELLS>& S = *reinterpret_cast<MeSmem<CELLS>*>(smem_raw);
+  __shared__ int unit_slot;
   const int tid = threadIdx.x;
-  const int unit = blockIdx.x;
+  int unit, iter = 0;
+  while (take_unit(w, unit, iter, &unit_slot)) {
   const int jb = job_of(w, unit);
   const FrameJob& job = jobs[jb];
   const int cols = job.fcols[level], rows = job.frows[level], ncell = cols * rows;
@@ -267,18 +273,38 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
     job.field[r][level][cell0 + tid] = pack_mv(S.mvx[tid], S.mvy[tid]);
     if (job.stats) atomicAdd(job.stats + level, S.two[tid] ? 2ull : 1ull);
   }
+  }  // units
 }
 
-int me_units(int nrefs, int cols, int rows) { return nrefs * ((cols * rows + kMeCells - 1) / kMeCells); }
+int me_units(int nrefs, int cols, int rows, int cells) { return nrefs * ((cols * rows + cells - 1) / cells); }
 
-void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, cudaStream_t st) {
+template <int CELLS>
+static void launch_cells(const FrameJob* jobs, const WorkList& w, int level, cudaStream_t st) {
   const int units = w.prefix[w.njobs];
-  if (units <= 0) return;
-  k_me_level<<<units, kMeThreads, sizeof(MeSmem), st>>>(jobs, w, level);
+  const size_t smem = sizeof(MeSmem<CELLS>);
+  const int grid = w.queue ? persistent_grid((const void*)k_me_level<CELLS>, kMeThreads, smem, units) : units;
+  k_me_level<CELLS><<<grid, kMeThreads, smem, st>>>(jobs, w, level);
+}
+
+void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, int cells, cudaStream_t st) {
+  if (w.prefix[w.njobs] <= 0) return;
+  if (cells == 16)
+    launch_cells<16>(jobs, w, level, st);
+  else
+    launch_cells<32>(jobs, w, level, st);
+}
+
+template <int CELLS>
+static cudaError_t attributes_cells() {
+  const size_t smem = sizeof(MeSmem<CELLS>);
+  const cudaError_t e = cudaFuncSetAttribute(k_me_level<CELLS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess) persistent_grid((const void*)k_me_level<CELLS>, kMeThreads, smem, 1);  // fills the grid cache
+  return e;
 }
 
 cudaError_t me_attributes() {
-  return cudaFuncSetAttribute(k_me_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MeSmem));
+  const cudaError_t e = attributes_cells<16>();
+  return e != cudaSuccess ? e : attributes_cells<32>();
 }
 
 }  // namespace celv2cu

@@ -66,7 +66,13 @@ SIGNATURES = {
     "celv2_work_counters": (C.c_int, [C.c_void_p, C.POINTER(C.c_ulonglong), C.c_int]),
     "celv2_decide_key_noalloc": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_void_p,
                                            C.c_void_p]),
+    "celv2_launch_multi": (C.c_int, [C.c_int, C.POINTER(C.c_void_p), C.POINTER(C.c_longlong), C.POINTER(C.c_int),
+                                     C.POINTER(C.POINTER(C.c_longlong)), C.POINTER(C.c_int64), C.c_int]),
+    "celv2_set_config": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "celv2_get_config": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
 }
+
+CFG_PERSISTENT, CFG_GRAPHS, CFG_PERSISTENT_OFF, CFG_INTER_CHUNK, CFG_ME_CELLS_L0 = 1, 2, 3, 4, 10
 
 STAGE_NAMES = ["upload+pyramid", "phases", "me_l4", "me_l3", "me_l2", "me_l1", "me_l0", "intra", "inter",
                "finalize"]
@@ -294,6 +300,14 @@ class CudaEngine:
     def clear_store(self) -> None:
         _check(library().celv2_clear_store(self._h))
 
+    def set_config(self, key: int, value: int) -> None:
+        _check(library().celv2_set_config(self._h, key, int(value)))
+
+    def get_config(self, key: int) -> int:
+        v = C.c_int()
+        _check(library().celv2_get_config(self._h, key, C.byref(v)))
+        return v.value
+
     def kernel_launches(self) -> int:
         return int(library().celv2_kernel_launches(self._h))
 
@@ -340,6 +354,20 @@ class CudaEngine:
         out = np.zeros((self.sb_cols * self.sb_rows, 7, 425, 2), np.int32)
         _check(library().celv2_debug_inter(self._h, out.ctypes.data_as(C.POINTER(C.c_int32))))
         return out
+
+
+def launch_multi(jobs, qindex, to_host: bool = False) -> None:
+    """One batch over engines of different frame sizes: jobs = [(engine, src_key, [ref keys])].
+    Each engine's records come back with engine.group_records(k) for its k-th job here."""
+    n = len(jobs)
+    qs = qindex if isinstance(qindex, (list, tuple)) else [qindex] * n
+    engs = (C.c_void_p * n)(*[e._h.value if isinstance(e._h, C.c_void_p) else e._h for e, _, _ in jobs])
+    sk = (C.c_longlong * n)(*[s for _, s, _ in jobs])
+    nr = (C.c_int * n)(*[len(r) for _, _, r in jobs])
+    rows = [(C.c_longlong * max(1, len(r)))(*r) for _, _, r in jobs]
+    rk = (C.POINTER(C.c_longlong) * n)(*[C.cast(r, C.POINTER(C.c_longlong)) for r in rows])
+    lams = (C.c_int64 * n)(*[_lam.lambda_q8(q) for q in qs])
+    _check(library().celv2_launch_multi(n, engs, sk, nr, rk, lams, 1 if to_host else 0))
 
 
 def int_peak(device: int = 0) -> float:

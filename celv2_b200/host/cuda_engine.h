@@ -1,7 +1,7 @@
 // cuda_engine.h: the B200 decision engine as a DecisionEngine of the reference encoder.
 //
 // A drop-in third engine next to CpuEngine and VulkanEngine (src/gpu/decision_engine.h:9-51),
-// selected as Device::Cuda / --device cuda. It forwards to the C ABI of
+// selected as Device::Cuda / --device cuda in make_engine (src/pipeline.cpp:43-72). It forwards to the C ABI of
 // include/celv2_cuda.h and converts the device records with the encoder's own
 // celv2::sb_out_to_decision (src/gpu/decision_map.cpp:65-105), whose SbOut layout the records
 // keep byte for byte. Compiled inside the reference tree: it includes "gpu/decision_engine.h".

@@ -6,7 +6,7 @@
  * quarter-pel refinement, intra / inter / compound SATD scoring and the bottom-up partition
  * choice -- and emits the decision records of include/celv2_decision.h, byte-identical to the
  * reference CpuEngine's decisions on the same 8-bit luma planes and lambda. Plain pointers and
- * sizes only; a C++ adapter deriving from DecisionEngine sits on top.
+ * sizes only; a C++ adapter deriving from DecisionEngine sits on top (celv2_b200/host/cuda_engine.h).
  *
  * Every function returns 0 on success and a negative CELV2_E* code on failure, with a message
  * for the calling thread in celv2_last_error(). One thread drives launch / prepare of an engine;
@@ -100,6 +100,14 @@ int celv2_upload(celv2_engine* e, const celv2_frame* f, long long key);
 int celv2_launch_group(celv2_engine* e, int njobs, const long long* src_keys, const int* nrefs,
                        const long long* const* ref_keys, const int64_t* lambda_q8, int to_host);
 int celv2_reserve_group(celv2_engine* e, int frames);
+/* The same across engines of different frame sizes on one GPU (frames of several streams): job i
+ * decides a frame of engines[i]'s store. One launch per stage for all of them -- each stage a
+ * persistent kernel draining one work queue, the largest jobs first -- on engines[0]'s stream.
+ * Engine e's jobs take its group slots in their order here (celv2_group_records(e, k) is e's k-th
+ * job). No counterpart in the reference, whose engines are each made for one frame size
+ * (src/vk/vk_engine.h:18). */
+int celv2_launch_multi(int njobs, celv2_engine* const* engines, const long long* src_keys, const int* nrefs,
+                       const long long* const* ref_keys, const int64_t* lambda_q8, int to_host);
 int celv2_group_records(celv2_engine* e, int job, const celv2_sb_out** records);
 
 /* Drops every frame of the store. */
@@ -130,6 +138,29 @@ int celv2_debug_intra(celv2_engine* e, int32_t* out);
 int celv2_debug_inter(celv2_engine* e, int32_t* out);
 /* Kernel launches the engine has issued so far (all stages). */
 long long celv2_kernel_launches(const celv2_engine* e);
+
+/* ---- Configuration ----
+ * How the stages run; none of it changes a decision.
+ *  CELV2_CFG_PERSISTENT: 1 (default) -- each stage is one persistent kernel whose CTAs drain a
+ *    device-side queue of the batch's work units (superblocks, cell groups); 0 -- one CTA per unit.
+ *  CELV2_CFG_GRAPHS: 1 -- celv2_launch_group captures a batch's whole stage sequence (descriptor
+ *    copy, queue reset, stage kernels, record copies) as a CUDA graph once per batch shape (the
+ *    jobs' reference counts) and replays it; 0 (default) -- launches stage by stage.
+ *  CELV2_CFG_PERSISTENT_OFF: a bit mask of stages that run one CTA per unit even when
+ *    CELV2_CFG_PERSISTENT is on (bit l: motion-search level l, 5 intra, 6 inter, 7 finalize).
+ *  CELV2_CFG_INTER_CHUNK: distinct MVs per pass of the inter stage, 8..64 (default 64).
+ *  CELV2_CFG_ME_CELLS_L0 + l: 8x8 cells per motion-search CTA at pyramid level l, 16 or 32
+ *    (default 32).
+ * The autotuner (celv2_b200/tune.py) times these per frame size and sets the fastest. */
+enum {
+  CELV2_CFG_PERSISTENT = 1,
+  CELV2_CFG_GRAPHS = 2,
+  CELV2_CFG_PERSISTENT_OFF = 3,
+  CELV2_CFG_INTER_CHUNK = 4,
+  CELV2_CFG_ME_CELLS_L0 = 10,
+};
+int celv2_set_config(celv2_engine* e, int key, int value);
+int celv2_get_config(const celv2_engine* e, int key, int* value);
 
 /* ---- Measurement ---- */
 
