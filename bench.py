@@ -13,8 +13,9 @@ reference's tools/engine_bench.cpp does). A step decides all 17 frames.
 Lines (one JSON line on rank 0):
   value  -- frames/s with the frames resident in HBM (uploaded before timing), CUDA events on the
             engine's stream, max over ranks; the leaves run as one batched launch per stage.
-  e2e    -- frames/s through the reference-facing API (launch / prepare / collect per frame, host
-            10-bit planes in, decision records back to host memory), wall clock.
+  e2e    -- frames/s end to end through the public API (host 10-bit planes in, decision records back
+            in host memory every step), wall clock: the mini-GOP through decide_group, with the
+            per-group-synchronous and the reference's per-frame launch/prepare/collect figures beside.
   roofline, cpu_baseline, clocks, gpu_launches as the harness asks.
 --impl reference times the reference's own CpuEngine (compiled from its sources into oracle/_ref)
 on the host cores, one 7-reference frame of the same workload per step.
@@ -319,6 +320,73 @@ def stage_bytes(plan, steps):
     return out
 
 
+def run_e2e(eng, clip, plan, steps, dist, local, world):
+    """Frames/s end to end through the public API, wall clock around whole steps, max over ranks.
+    Every step uploads its 17 frames from host 10-bit planes (new keys: new pictures) and brings
+    every record back into host memory.
+      value     -- the mini-GOP through CudaEngine.decide_group (celv2_upload, celv2_set_output,
+                   celv2_launch_group): groups issued back to back, the records copied straight into
+                   the DecisionMaps while the next group runs; the step ends when all are in host
+                   memory.
+      per_group -- the same, waiting for each group's records before the next group is issued.
+      per_frame -- the reference's own interface: launch / prepare / collect per frame (celv2_launch,
+                   celv2_prepare, celv2_wait_row), every reference uploaded once per step."""
+    from celv2_b200 import engine as E
+    from celv2_b200.records import DecisionMap
+
+    nsb = eng.sb_cols * eng.sb_rows
+    plane = clip[0].hy.nbytes
+
+    def timed(run):
+        run(0)  # warm: pools, graphs
+        eng.finish()
+        barrier(dist, local)
+        t0 = time.perf_counter()
+        for s in range(steps):
+            run(s + 1)
+        eng.finish()
+        dt = max_over_ranks(time.perf_counter() - t0, dist, local)
+        return NFRAMES * steps * world / dt
+
+    def groups(s, wait):
+        key = lambda d: s * 1000 + d  # noqa: E731 -- new pictures every step (reconstructions differ)
+        maps = []
+        for group in plan:
+            maps += eng.decide_group([clip[src].hy for src, _ in group],
+                                     [[clip[r].hy for r in refs] for _, refs in group], QINDEX,
+                                     ref_keys=[[key(r) for r in refs] for _, refs in group], wait=wait)
+        return maps
+
+    def frames(s):
+        order = [(src, refs) for group in plan for src, refs in group]
+        key = lambda d: 1_000_000 + s * 1000 + d  # noqa: E731 -- apart from the group runs' keys
+        for i, (src, refs) in enumerate(order):
+            dm = DecisionMap()
+            eng.launch(clip[src].hy, [clip[r].hy for r in refs], QINDEX, dm, [key(r) for r in refs], key(src))
+            if i + 1 < len(order):
+                eng.prepare(clip[order[i + 1][0]].hy, key(order[i + 1][0]))
+            eng.collect(dm, E.RowGate())
+
+    held = []  # the maps of a step stay alive until its records are read (decide_group, wait=False)
+
+    def pipelined_step(s):
+        held.clear()
+        held.extend(groups(s, False))
+        eng.finish()  # the step's records are all in host memory
+
+    pipelined = timed(pipelined_step)
+    per_group = timed(lambda s: groups(s, True))
+    per_frame = timed(frames)
+    ref_frames = {r for group in plan for _, refs in group for r in refs}
+    return {"value": pipelined, "unit": UNIT, "h2d_bytes_per_step": (NFRAMES + len(ref_frames)) * plane,
+            "d2h_bytes_per_step": NFRAMES * nsb * RECORD_BYTES, "steps": steps,
+            "api": "CudaEngine.decide_group per coding group (celv2_upload, celv2_set_output, celv2_launch_group); "
+                   "records straight into host DecisionMaps, copies overlapping the next group",
+            "per_group": {"value": per_group, "note": "each group's records in host memory before the next group"},
+            "per_frame": {"value": per_frame, "h2d_bytes_per_step": (NFRAMES + len(ref_frames)) * plane,
+                          "api": "launch/prepare/collect per frame (celv2_launch, celv2_prepare, celv2_wait_row)"}}
+
+
 def run_cuda_arm(args):
     import torch
 
@@ -377,27 +445,8 @@ def run_cuda_arm(args):
     dominant = max(st, key=lambda k: st[k][0])
     dom_ms, dom_n = st[dominant]
 
-    # e2e through the reference-facing API: host 10-bit planes in, records to host memory
-    e2e_steps = max(1, min(args.steps, 3))
-    h2d = d2h = 0
-    barrier(dist, local)
-    t0 = time.perf_counter()
-    for s in range(e2e_steps):
-        order = [(src, refs) for group in plan for src, refs in group]
-        key = lambda d: (s + 1) * 1000 + d  # noqa: E731 -- new pictures every step (reconstructions differ)
-        for i, (src, refs) in enumerate(order):
-            dm = DecisionMap()
-            eng.launch(clip[src].hy, [clip[r].hy for r in refs], QINDEX, dm, [key(r) for r in refs], key(src))
-            if i + 1 < len(order):
-                eng.prepare(clip[order[i + 1][0]].hy, key(order[i + 1][0]))
-            eng.collect(dm, E.RowGate())
-    t_e2e = time.perf_counter() - t0
-    t_e2e = max_over_ranks(t_e2e, dist, local)
-    plane = clip[0].hy.nbytes
-    ref_frames = {r for group in plan for _, refs in group for r in refs}
-    h2d = (NFRAMES + len(ref_frames)) * plane
-    d2h = NFRAMES * eng.sb_cols * eng.sb_rows * 38872
-    e2e = NFRAMES * e2e_steps * world / t_e2e
+    # e2e: host 10-bit planes in, decision records back in host memory, every step
+    e2e = run_e2e(eng, clip, plan, max(1, min(args.steps, 5)), dist, local, world)
 
     line = None
     if rank == 0:
@@ -445,8 +494,7 @@ def run_cuda_arm(args):
                            "launch": {"persistent_queue_kernels": True, "cuda_graphs": not args.no_graphs,
                                       "tuned": {k: v for k, v in (tuned or {}).items() if k != "stage_ms"}}},
                 "clocks": clocks.summary(), "gpu_launches": launches,
-                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "steps": e2e_steps, "api": "launch/prepare/collect per frame (celv2_launch, celv2_wait_row)"},
+                "e2e": e2e,
                 "roofline": roofline, "cpu_baseline": cpu}
         print(json.dumps(line))
     eng.close()
@@ -475,7 +523,7 @@ def run_profile_case(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -145,6 +145,50 @@ __device__ __forceinline__ int satd4_bytes(const uint32_t* ce, const uint32_t* c
   return 2 * sum;
 }
 
+// dp4a with unsigned bytes a and signed bytes b: c + sum_k a_k * b_k.
+__device__ __forceinline__ int dp4a_us(uint32_t a, uint32_t b, int c) {
+  int d;
+  asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+  return d;
+}
+
+// The four 1-D Walsh-Hadamard basis rows of length 4 as signed bytes (column 0 in the low byte):
+// (1,1,1,1), (1,-1,1,-1), (1,1,-1,-1), (1,-1,-1,1) -- the rows hadamard4x4's row butterflies form.
+__device__ __forceinline__ uint32_t wh_row(int k) {
+  return k == 0 ? 0x01010101u : k == 1 ? 0xFF01FF01u : k == 2 ? 0xFFFF0101u : 0x01FFFF01u;
+}
+
+// The same rows negated.
+__device__ __forceinline__ uint32_t wh_row_neg(int k) {
+  return k == 0 ? 0xFFFFFFFFu : k == 1 ? 0x01FF01FFu : k == 2 ? 0x0101FFFFu : 0xFF0101FFu;
+}
+
+// Row-transformed cur tile for satd4_rows: C[4k + i] = <row i of the tile, basis row k>.
+__device__ __forceinline__ void wh_rows_cur(const uint32_t* c, int* C) {
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+#pragma unroll
+    for (int i = 0; i < 4; i++) C[4 * k + i] = dp4a_us(c[i], wh_row(k), 0);
+}
+
+// hadamard4x4 of the residual cur - pred of a 4x4 tile from the row-transformed cur tile C and the
+// prediction rows p (packed bytes): each residual row coefficient is one dp4a of the prediction
+// row with the negated basis row, accumulated onto cur's; the column butterflies follow, the last
+// one folded with the absolute values into |x + y| + |x - y| = 2 max(|x|, |y|). The same sum of
+// 16 absolute coefficients.
+__device__ __forceinline__ int satd4_rows(const int* C, const uint32_t* p) {
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t neg = wh_row_neg(k);
+    const int r0 = dp4a_us(p[0], neg, C[4 * k]), r1 = dp4a_us(p[1], neg, C[4 * k + 1]);
+    const int r2 = dp4a_us(p[2], neg, C[4 * k + 2]), r3 = dp4a_us(p[3], neg, C[4 * k + 3]);
+    const int s01 = r0 + r1, d01 = r0 - r1, s23 = r2 + r3, d23 = r2 - r3;
+    sum += max(abs(s01), abs(s23)) + max(abs(d01), abs(d23));
+  }
+  return 2 * sum;
+}
+
 // Residual of one 4x4 row: four cur bytes minus four prediction bytes.
 __device__ __forceinline__ void residual_row(int* d, uint32_t c, uint32_t p) {
   d[0] = (int)(c & 255) - (int)(p & 255);

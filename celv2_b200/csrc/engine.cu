@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -152,6 +153,12 @@ struct Slot {
   long long key = -1;
   long long used = -1;
   bool phases = false;
+  bool resident = false;  // uploaded into the store (celv2_upload): launch()'s reference cache leaves it
+  // Store uploads run on the engine's upload stream: `ready` marks this slot's upload done; the
+  // launches that read the slot record `last_use` on their stream, which a later upload into the
+  // slot waits for.
+  cudaEvent_t ready = nullptr, last_use = nullptr;
+  bool ready_pending = false, use_pending = false;
   uint8_t* mem = nullptr;
   size_t bytes = 0;
   DevPyramid pyr{};
@@ -175,6 +182,7 @@ struct JobBuffers {
   int* intra = nullptr;      // nsb * kBlocks * kModes
   int2* inter = nullptr;     // nsb * kMaxRefs * kBlocks
   celv2_sb_out* out = nullptr;
+  celv2_sb_out* out2 = nullptr;  // group buffers: the records of every other group (see group_parity)
 };
 
 }  // namespace
@@ -193,6 +201,11 @@ struct celv2_engine {
   JobBuffers single;             // the launch() path
   int* intra_prep[2] = {nullptr, nullptr};  // intra SATDs per source slot
   celv2_sb_out* host_out = nullptr;          // pinned, nsb records
+  // caller memory for the next launch's records (celv2_set_output), per job; where the last
+  // launch's records went (launch: last_out; group: group_out[job])
+  celv2_sb_out* next_out[kMaxJobs] = {};
+  celv2_sb_out* last_out = nullptr;
+  celv2_sb_out* group_out[kMaxJobs] = {};
   std::vector<cudaEvent_t> row_done;
   std::vector<int> order;
   int row_streams = 1;
@@ -211,6 +224,13 @@ struct celv2_engine {
   std::vector<JobBuffers> group;
   celv2_sb_out* group_host = nullptr;
   int group_jobs = 0;
+  // Group records go to the host on copy_st, overlapping the next group's stages, which write the
+  // other of two device record buffers (group_parity); copied[p] marks buffer p's copies done.
+  cudaStream_t copy_st = nullptr;
+  cudaStream_t up_st = nullptr;  // celv2_upload's stream (frame-store uploads)
+  cudaEvent_t stages_done = nullptr, copied[2] = {nullptr, nullptr};
+  bool copy_pending[2] = {false, false};
+  int group_parity = 0;
   long long kernel_launches = 0;
   // stage timing: an event pair around each stage launch, harvested when the stream is idle
   bool timing = false;
@@ -268,8 +288,10 @@ struct celv2_engine {
     cudaSetDevice(device);
     if (st) cudaStreamSynchronize(st);
     if (prep_st) cudaStreamSynchronize(prep_st);
+    if (copy_st) cudaStreamSynchronize(copy_st);
+    if (up_st) cudaStreamSynchronize(up_st);
     free_graphs();
-    for (Slot* s : store) cudaFree(s->mem), delete s;
+    for (Slot* s : store) free_slot(s);
     for (Slot& s : srcs) cudaFree(s.mem);
     for (Stage& s : stages) {
       cudaFreeHost(s.host), cudaFree(s.dev);
@@ -290,12 +312,24 @@ struct celv2_engine {
     for (cudaEvent_t e : ring_done)
       if (e) cudaEventDestroy(e);
     if (prep_done) cudaEventDestroy(prep_done);
+    if (stages_done) cudaEventDestroy(stages_done);
+    for (cudaEvent_t e : copied)
+      if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
     if (prep_st) cudaStreamDestroy(prep_st);
+    if (copy_st) cudaStreamDestroy(copy_st);
+    if (up_st) cudaStreamDestroy(up_st);
+  }
+
+  static void free_slot(Slot* s) {
+    cudaFree(s->mem);
+    if (s->ready) cudaEventDestroy(s->ready);
+    if (s->last_use) cudaEventDestroy(s->last_use);
+    delete s;
   }
 
   static void free_buffers(JobBuffers& b) {
-    cudaFree(b.fields), cudaFree(b.intra), cudaFree(b.inter), cudaFree(b.out);
+    cudaFree(b.fields), cudaFree(b.intra), cudaFree(b.inter), cudaFree(b.out), cudaFree(b.out2);
     b = JobBuffers{};
   }
 
@@ -304,6 +338,7 @@ struct celv2_engine {
     if (with_intra) CK(cudaMalloc(&b.intra, (size_t)g.nsb * kBlocks * kModes * sizeof(int)));
     CK(cudaMalloc(&b.inter, (size_t)g.nsb * kMaxRefs * kBlocks * sizeof(int2)));
     CK(cudaMalloc(&b.out, (size_t)g.nsb * sizeof(celv2_sb_out)));
+    if (with_intra) CK(cudaMalloc(&b.out2, (size_t)g.nsb * sizeof(celv2_sb_out)));
   }
 
   void init(int width, int height, int dev) {
@@ -314,6 +349,10 @@ struct celv2_engine {
     CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&prep_st, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&prep_done, cudaEventDisableTiming));
+    CK(cudaStreamCreateWithFlags(&copy_st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&up_st, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&stages_done, cudaEventDisableTiming));
+    for (cudaEvent_t& e : copied) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     CK(cudaMalloc(&djobs, kRingJobs * sizeof(FrameJob)));
     CK(cudaMalloc(&queues, 16 * sizeof(unsigned)));
     CK(cudaMallocHost(&ring, (size_t)kRing * kRingJobs * sizeof(FrameJob)));
@@ -321,6 +360,7 @@ struct celv2_engine {
     alloc_buffers(single, false);
     for (int*& p : intra_prep) CK(cudaMalloc(&p, (size_t)g.nsb * kBlocks * kModes * sizeof(int)));
     CK(cudaMallocHost(&host_out, (size_t)g.nsb * sizeof(celv2_sb_out)));
+    last_out = host_out;
     row_done.resize(g.sb_rows);
     for (cudaEvent_t& e : row_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     stages.resize(16);
@@ -374,8 +414,10 @@ struct celv2_engine {
 
   // Copies f's luma into pinned memory (synchronously: the caller may change it afterwards), then
   // queues its upload, the 8-bit level 0, the pyramid and (phases) the quarter-pel planes.
-  void upload(const celv2_frame* f, Slot& s, bool phases, cudaStream_t stream) {
-    alloc_slot(s, phases || s.phases);
+  // Uploads f into s on `stream`: 8-bit level 0 and pyramid, the phase planes too when `phases`
+  // (room for them when `room`).
+  void upload(const celv2_frame* f, Slot& s, bool phases, cudaStream_t stream, bool room = false) {
+    alloc_slot(s, phases || room || s.phases);
     const bool wide = f->y == nullptr;
     const int pitch = f->pitch ? f->pitch : g.pw;
     const size_t row = (size_t)g.pw * (wide ? 2 : 1);
@@ -417,7 +459,7 @@ struct celv2_engine {
         if (s->key == key) return s;
     Slot* pick = nullptr;
     for (Slot* s : store) {
-      if (s->used == now) continue;
+      if (s->used == now || s->resident) continue;
       bool needed = false;
       for (int i = 0; i < nkeys && keys; i++) needed |= s->key >= 0 && s->key == keys[i];
       if (needed) continue;
@@ -512,7 +554,9 @@ struct celv2_engine {
   }
 
   void wait_idle() {
+    CK(cudaStreamSynchronize(up_st));
     CK(cudaStreamSynchronize(st));
+    CK(cudaStreamSynchronize(copy_st));
     pending = false;
     if (!timed.empty()) {
       CK(cudaStreamSynchronize(prep_st));
@@ -522,6 +566,8 @@ struct celv2_engine {
 
   void launch(const celv2_frame* src, const celv2_frame* refs, int nrefs, long long lam, const long long* keys,
               long long src_key) {
+    celv2_sb_out* dest = take_outputs()[0];  // this launch's, even when it fails
+    if (!dest) dest = host_out;
     check_frame(src, "source");
     if (nrefs < 0 || nrefs > kMaxRefs) invalid("CudaEngine: too many references");
     for (int r = 0; r < nrefs; r++) check_frame(&refs[r], "reference");
@@ -548,9 +594,11 @@ struct celv2_engine {
         bool fresh;
         Slot* s = ref_slot(keys ? keys[r] : -1, keys, keys ? nrefs : 0, now, fresh);
         if (fresh) {
+          wait_ready(*s, st);  // a dropped store frame's upload may still run
           upload(&refs[r], *s, true, st);
           s->key = keys ? keys[r] : -1;
         } else {
+          wait_ready(*s, st);  // a frame of the store
           make_phases(*s, st);
         }
         s->used = now;
@@ -559,6 +607,7 @@ struct celv2_engine {
       std::vector<FrameJob> jobs(1);
       fill_job(jobs[0], srcs[use].pyr, used, nrefs, single, intra_prep[use], lam);
       run_stages(jobs, !prepared, st);
+      mark_used(used, nrefs, st);
       last_nrefs = nrefs;
       // rows back to the host in row-stream order
       const int streams = std::max(1, std::min(row_streams, g.sb_rows));
@@ -569,10 +618,11 @@ struct celv2_engine {
           if (s * run + i < g.sb_rows) order.push_back(s * run + i);
       for (int r : order) {
         const size_t first = (size_t)r * g.sb_cols;
-        CK(cudaMemcpyAsync(host_out + first, single.out + first, g.sb_cols * sizeof(celv2_sb_out),
+        CK(cudaMemcpyAsync(dest + first, single.out + first, g.sb_cols * sizeof(celv2_sb_out),
                            cudaMemcpyDeviceToHost, st));
         CK(cudaEventRecord(row_done[r], st));
       }
+      last_out = dest;
       pending = true;
     } catch (...) {
       cudaStreamSynchronize(st);  // a failure leaves no work running
@@ -613,7 +663,26 @@ struct celv2_engine {
     if (row < 0 || row >= g.sb_rows) invalid("row out of range");
     if (!pending && launches == 0) throw Error(CELV2_ESTATE, "no launch to collect");
     CK(cudaEventSynchronize(row_done[row]));
-    return host_out + (size_t)row * g.sb_cols;
+    return last_out + (size_t)row * g.sb_cols;
+  }
+
+  // The caller memory named for the next launch's jobs (null: the engine's buffer); clears it.
+  std::array<celv2_sb_out*, kMaxJobs> take_outputs() {
+    std::array<celv2_sb_out*, kMaxJobs> o;
+    for (int j = 0; j < kMaxJobs; j++) o[j] = next_out[j], next_out[j] = nullptr;
+    return o;
+  }
+
+  // The device record buffer set (0: out, 1: out2) of the next group, after `stream` waits for the
+  // host copies that still read it (two groups back).
+  int take_parity(cudaStream_t stream) {
+    const int par = group_parity;
+    group_parity ^= 1;
+    if (copy_pending[par]) {
+      CK(cudaStreamWaitEvent(stream, copied[par], 0));
+      copy_pending[par] = false;
+    }
+    return par;
   }
 
   // ---- group path ----
@@ -621,6 +690,7 @@ struct celv2_engine {
     if (frames <= group_cap) return;
     wait_idle();
     free_graphs();  // they hold the old buffers' addresses
+    group_jobs = 0;  // the last group's records go with the old host buffer
     for (JobBuffers& b : group) free_buffers(b);
     group.assign(frames, JobBuffers{});
     for (JobBuffers& b : group) alloc_buffers(b, true);
@@ -638,23 +708,54 @@ struct celv2_engine {
   void upload_store(const celv2_frame* f, long long key) {
     check_frame(f, "frame");
     if (key < 0) invalid("store keys must be >= 0");
-    if (pending) wait_idle();
+    // No wait for queued work: it runs on this stream, ahead of the upload.
     Slot* s = find(key);
+    if (!s)  // a dropped store frame's memory (it has the events), the least recently used
+      for (Slot* x : store)
+        if (x->key < 0 && !x->resident && x->last_use && (!s || x->used < s->used)) s = x;
     if (!s) {
       s = new Slot;
       store.push_back(s);
     }
+    if (!s->ready) {
+      CK(cudaEventCreateWithFlags(&s->ready, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&s->last_use, cudaEventDisableTiming));
+    }
     s->key = -1;
-    upload(f, *s, true, st);
+    // on the upload stream, after the queued work that reads the slot's old contents; the phase
+    // planes are made by the first launch that uses the frame as a reference
+    if (s->use_pending) CK(cudaStreamWaitEvent(up_st, s->last_use, 0));
+    s->use_pending = false;
+    upload(f, *s, false, up_st, true);
+    CK(cudaEventRecord(s->ready, up_st));
+    s->ready_pending = true;
     s->key = key;
     s->used = launches;
+    s->resident = true;
+  }
+
+  // `stream` waits for s's store upload, if one is in flight.
+  void wait_ready(Slot& s, cudaStream_t stream) {
+    if (s.ready_pending) CK(cudaStreamWaitEvent(stream, s.ready, 0));
+  }
+
+  // The slots a launch on `stream` reads: a later upload into them waits for this point.
+  void mark_used(Slot* const* slots, int n, cudaStream_t stream) {
+    for (int i = 0; i < n; i++) {
+      Slot* x = slots[i];
+      if (!x->last_use) continue;  // not a store slot (launch()'s own cache, on this stream)
+      CK(cudaEventRecord(x->last_use, stream));
+      x->use_pending = true;
+    }
   }
 
   void launch_group(int njobs, const long long* src_keys, const int* nrefs, const long long* const* ref_keys,
                     const int64_t* lams, bool to_host) {
+    const std::array<celv2_sb_out*, kMaxJobs> dests = take_outputs();
     if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per group");
     if (njobs > group_cap) reserve_group(std::max(njobs, 8));
     std::vector<FrameJob> jobs(njobs);
+    std::vector<Slot*> reads;
     for (int j = 0; j < njobs; j++) {
       Slot* cur = find(src_keys[j]);
       if (!cur) invalid("group: no stored frame with the source key");
@@ -664,18 +765,34 @@ struct celv2_engine {
       for (int r = 0; r < nrefs[j]; r++) {
         refs[r] = find(ref_keys[j][r]);
         if (!refs[r]) invalid("group: no stored frame with a reference key");
+      }
+      wait_ready(*cur, st);
+      reads.push_back(cur);
+      for (int r = 0; r < nrefs[j]; r++) {
+        wait_ready(*refs[r], st);
         make_phases(*refs[r], st);
+        reads.push_back(refs[r]);
       }
       fill_job(jobs[j], cur->pyr, refs, nrefs[j], group[j], group[j].intra, lams[j]);
     }
-    if (use_graphs && !timing) {
-      launch_graph(jobs, to_host);
-    } else {
+    const int par = take_parity(st);
+    for (int j = 0; j < njobs; j++) jobs[j].out = par ? group[j].out2 : group[j].out;
+    if (use_graphs && !timing)
+      launch_graph(jobs);
+    else
       run_stages(jobs, true, st);
-      if (to_host)
-        for (int j = 0; j < njobs; j++)
-          CK(cudaMemcpyAsync(group_host + (size_t)j * g.nsb, group[j].out, g.nsb * sizeof(celv2_sb_out),
-                             cudaMemcpyDeviceToHost, st));
+    mark_used(reads.data(), (int)reads.size(), st);
+    if (to_host) {
+      CK(cudaEventRecord(stages_done, st));
+      CK(cudaStreamWaitEvent(copy_st, stages_done, 0));
+      for (int j = 0; j < njobs; j++) {
+        group_out[j] = dests[j] ? dests[j] : group_host + (size_t)j * g.nsb;
+        CK(cudaMemcpyAsync(group_out[j], jobs[j].out, g.nsb * sizeof(celv2_sb_out), cudaMemcpyDeviceToHost, copy_st));
+      }
+      CK(cudaEventRecord(copied[par], copy_st));
+      copy_pending[par] = true;
+    } else {
+      for (int j = 0; j < njobs; j++) group_out[j] = group_host + (size_t)j * g.nsb;
     }
     group_jobs = njobs;
     ++launches;
@@ -684,7 +801,7 @@ struct celv2_engine {
 
   // ---- CUDA graphs: a batch's whole stage sequence captured once per shape, then replayed ----
   struct Graph {
-    std::vector<int> key;  // to_host, then each job's reference count
+    std::vector<int> key;  // each job's reference count
     cudaGraphExec_t exec = nullptr;
     FrameJob* host_jobs = nullptr;  // pinned: the replay's descriptor copy reads it
     cudaEvent_t done = nullptr;
@@ -703,8 +820,8 @@ struct celv2_engine {
     graphs.clear();
   }
 
-  void launch_graph(const std::vector<FrameJob>& jobs, bool to_host) {
-    std::vector<int> key{to_host ? 1 : 0};
+  void launch_graph(const std::vector<FrameJob>& jobs) {
+    std::vector<int> key;
     for (const FrameJob& j : jobs) key.push_back(j.nrefs);
     Graph* gr = nullptr;
     for (Graph& x : graphs)
@@ -721,10 +838,6 @@ struct celv2_engine {
       try {
         CK(cudaMemcpyAsync(djobs, gr->host_jobs, n * sizeof(FrameJob), cudaMemcpyHostToDevice, st));
         gr->kernels = enqueue_stages(jobs, true, st);
-        if (to_host)
-          for (int j = 0; j < n; j++)
-            CK(cudaMemcpyAsync(group_host + (size_t)j * g.nsb, group[j].out, g.nsb * sizeof(celv2_sb_out),
-                               cudaMemcpyDeviceToHost, st));
       } catch (...) {
         cudaStreamEndCapture(st, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -751,20 +864,24 @@ namespace {
 // the first engine's stream. Engine e's jobs take its group slots in order of appearance.
 void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_keys, const int* nrefs,
                   const long long* const* ref_keys, const int64_t* lams, bool to_host) {
-  if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per batch");
   celv2_engine* lead = engines[0];
   std::vector<celv2_engine*> uniq;
+  for (int j = 0; j < std::min(njobs, kMaxJobs); j++)
+    if (engines[j] && std::find(uniq.begin(), uniq.end(), engines[j]) == uniq.end()) uniq.push_back(engines[j]);
+  // the caller memory named for this launch, which takes it even when it fails
+  std::vector<std::array<celv2_sb_out*, kMaxJobs>> dests;
+  for (celv2_engine* e : uniq) dests.push_back(e->take_outputs());
+  if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per batch");
   for (int j = 0; j < njobs; j++) {
     if (!engines[j]) invalid("null engine");
     if (engines[j]->device != lead->device) invalid("a batch runs on one GPU");
-    if (std::find(uniq.begin(), uniq.end(), engines[j]) == uniq.end()) uniq.push_back(engines[j]);
   }
   for (celv2_engine* e : uniq) {
     int count = 0;
     for (int j = 0; j < njobs; j++) count += engines[j] == e;
     if (count > e->group_cap) e->reserve_group(std::max(count, 8));
   }
-  // the stores' uploads first: the lead stream waits for every other engine's stream
+  // the other engines' queued work first: the lead stream waits for each of their streams
   for (celv2_engine* e : uniq)
     if (e != lead) {
       cudaEvent_t ev;
@@ -778,9 +895,13 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     celv2_engine* e;
     int slot;
     long long work;
+    celv2_sb_out* dest;  // the caller's memory for the records, or null
   };
+  std::vector<int> par;  // each engine's device record buffer set for this batch
+  for (celv2_engine* e : uniq) par.push_back(e->take_parity(lead->st));
   std::vector<Entry> entries;
   std::vector<int> next(uniq.size(), 0);
+  std::vector<std::vector<Slot*>> reads(uniq.size());  // each engine's store slots this batch reads
   for (int j = 0; j < njobs; j++) {
     celv2_engine* e = engines[j];
     const int ei = (int)(std::find(uniq.begin(), uniq.end(), e) - uniq.begin());
@@ -793,11 +914,18 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     for (int r = 0; r < nrefs[j]; r++) {
       refs[r] = e->find(ref_keys[j][r]);
       if (!refs[r]) invalid("batch: no stored frame with a reference key");
+    }
+    e->wait_ready(*cur, lead->st);
+    reads[ei].push_back(cur);
+    for (int r = 0; r < nrefs[j]; r++) {
+      e->wait_ready(*refs[r], lead->st);
       e->make_phases(*refs[r], lead->st);
+      reads[ei].push_back(refs[r]);
     }
     Entry en;
     e->fill_job(en.job, cur->pyr, refs, nrefs[j], e->group[slot], e->group[slot].intra, lams[j]);
-    en.e = e, en.slot = slot, en.work = (long long)(nrefs[j] + 1) * e->g.nsb;
+    en.job.out = par[ei] ? e->group[slot].out2 : e->group[slot].out;
+    en.e = e, en.slot = slot, en.work = (long long)(nrefs[j] + 1) * e->g.nsb, en.dest = dests[ei][slot];
     entries.push_back(en);
   }
   // the largest jobs first, so the queues' last units are small ones
@@ -805,10 +933,24 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
   std::vector<FrameJob> jobs;
   for (const Entry& en : entries) jobs.push_back(en.job);
   lead->run_stages(jobs, true, lead->st);
+  for (size_t i = 0; i < uniq.size(); i++) uniq[i]->mark_used(reads[i].data(), (int)reads[i].size(), lead->st);
+  if (to_host) {  // on the lead's copy stream, overlapping later work
+    CK(cudaEventRecord(lead->stages_done, lead->st));
+    CK(cudaStreamWaitEvent(lead->copy_st, lead->stages_done, 0));
+  }
+  for (const Entry& en : entries) {
+    celv2_sb_out* d = en.dest && to_host ? en.dest : en.e->group_host + (size_t)en.slot * en.e->g.nsb;
+    en.e->group_out[en.slot] = d;
+    if (to_host)
+      CK(cudaMemcpyAsync(d, en.job.out, en.e->g.nsb * sizeof(celv2_sb_out), cudaMemcpyDeviceToHost, lead->copy_st));
+  }
   if (to_host)
-    for (const Entry& en : entries)
-      CK(cudaMemcpyAsync(en.e->group_host + (size_t)en.slot * en.e->g.nsb, en.e->group[en.slot].out,
-                         en.e->g.nsb * sizeof(celv2_sb_out), cudaMemcpyDeviceToHost, lead->st));
+    for (size_t i = 0; i < uniq.size(); i++) {
+      celv2_engine* e = uniq[i];
+      CK(cudaEventRecord(e->copied[par[i]], lead->copy_st));
+      e->copy_pending[par[i]] = true;
+      if (e != lead) CK(cudaStreamWaitEvent(e->copy_st, e->copied[par[i]], 0));  // e's waits cover them
+    }
   // every engine's later work waits for this batch
   cudaEvent_t done;
   CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
@@ -864,8 +1006,11 @@ int celv2_launch(celv2_engine* e, const celv2_frame* src, const celv2_frame* ref
                  const long long* ref_keys, long long src_key) {
   return guarded([&] {
     if (!e) invalid("null engine");
+    if (nrefs > 0 && !refs) {
+      e->take_outputs();
+      invalid("null references");
+    }
     CK(cudaSetDevice(e->device));
-    if (nrefs > 0 && !refs) invalid("null references");
     e->launch(src, refs, nrefs, lambda_q8, ref_keys, src_key);
   });
 }
@@ -929,7 +1074,11 @@ int celv2_upload(celv2_engine* e, const celv2_frame* f, long long key) {
 int celv2_launch_group(celv2_engine* e, int njobs, const long long* src_keys, const int* nrefs,
                        const long long* const* ref_keys, const int64_t* lambda_q8, int to_host) {
   return guarded([&] {
-    if (!e || !src_keys || !nrefs || !lambda_q8) invalid("null argument");
+    if (!e) invalid("null engine");
+    if (!src_keys || !nrefs || !lambda_q8) {
+      e->take_outputs();  // named for this launch, which fails
+      invalid("null argument");
+    }
     CK(cudaSetDevice(e->device));
     e->launch_group(njobs, src_keys, nrefs, ref_keys, lambda_q8, to_host != 0);
   });
@@ -950,7 +1099,36 @@ int celv2_group_records(celv2_engine* e, int job, const celv2_sb_out** records) 
     if (job < 0 || job >= e->group_jobs) invalid("no such job in the last group");
     CK(cudaSetDevice(e->device));
     e->wait_idle();
-    *records = e->group_host + (size_t)job * e->g.nsb;
+    *records = e->group_out[job];
+  });
+}
+
+int celv2_set_output(celv2_engine* e, int job, celv2_sb_out* records) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    if (job < 0 || job >= kMaxJobs - 1) invalid("set_output: job out of range");
+    if (records) {
+      cudaPointerAttributes a{};
+      if (cudaPointerGetAttributes(&a, records) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        invalid("set_output: records must be page-locked host memory (celv2_host_alloc)");
+      }
+    }
+    e->next_out[job] = records;
+  });
+}
+
+int celv2_host_alloc(long long bytes, void** out) {
+  return guarded([&] {
+    if (!out || bytes <= 0) invalid("host_alloc: a positive size and an output pointer");
+    *out = nullptr;
+    CK(cudaHostAlloc(out, (size_t)bytes, cudaHostAllocPortable));
+  });
+}
+
+int celv2_host_free(void* p) {
+  return guarded([&] {
+    if (p) CK(cudaFreeHost(p));
   });
 }
 
@@ -959,8 +1137,15 @@ int celv2_clear_store(celv2_engine* e) {
     if (!e) invalid("null engine");
     CK(cudaSetDevice(e->device));
     e->wait_idle();
-    for (Slot* s : e->store) cudaFree(s->mem), delete s;
+    for (Slot* s : e->store) celv2_engine::free_slot(s);
     e->store.clear();
+  });
+}
+
+int celv2_drop_frame(celv2_engine* e, long long key) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    if (Slot* s = e->find(key)) s->key = -1, s->used = 0, s->resident = false;
   });
 }
 

@@ -198,14 +198,15 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
     }
   }
 
-  // this thread's tile: cur rows in registers as 16-bit lane pairs (the grid lies inside the margin)
+  // this thread's tile: its cur rows, row-transformed, in registers (the grid lies inside the margin)
   const int tx = tid & 15, ty = tid >> 4;
   const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
-  uint32_t ce[4], co[4];
+  int C[16];
+  {
+    uint32_t c[4];
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const uint32_t c = load4(cur.p + (long long)(oy + ty * 4 + i) * cur.stride + ox + tx * 4);
-    ce[i] = bytes_even(c), co[i] = bytes_odd(c);
+    for (int i = 0; i < 4; i++) c[i] = load4(cur.p + (long long)(oy + ty * 4 + i) * cur.stride + ox + tx * 4);
+    wh_rows_cur(c, C);
   }
   // chunks of equal size, at most `chunk` MVs each
   const int nchunks = (nd + chunk - 1) / chunk, csize = (nd + nchunks - 1) / nchunks;
@@ -236,7 +237,7 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
             for (int k = 0; k < 4; k++) pr[i] |= (uint32_t)at(ph, y + i, x + k) << (8 * k);
           }
         }
-        sat[h] = satd4_bytes(ce, co, pr);
+        sat[h] = satd4_rows(C, pr);
       }
 #pragma unroll
       for (int h = 0; h < 2; h++) {

@@ -34,6 +34,7 @@ template <int CELLS>
 struct MeSmem {
   static constexpr int kSearches = 2 * CELLS;  // at most two centres per cell
   uint32_t cur[CELLS][16];
+  int ccoef[CELLS][4][16];  // level 0: each 4x4 tile's row-transformed cur rows (satd4_rows)
   int csad[CELLS][6];
   int ccx[CELLS][6], ccy[CELLS][6];
   int scell[kSearches], sx[kSearches], sy[kSearches], soff[kSearches];
@@ -42,8 +43,15 @@ struct MeSmem {
   int mvx[CELLS], mvy[CELLS];
   int rsatd[CELLS][9];
   int nsearch;
-  uint32_t win[kSearches * kWinStride];
+  alignas(16) uint32_t win[kSearches * kWinStride];
 };
+
+// An asynchronous 8-byte global -> shared copy (cp.async; both addresses 8-byte aligned).
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gsrc) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // 4 bytes of a plane at (x .. x + 3, y), clamped like Plane::at where the row leaves the margin.
 __device__ __forceinline__ uint32_t row4(const DevPlane& s, int x, int y) {
@@ -82,8 +90,9 @@ __device__ __forceinline__ int sad8(const uint32_t* c, const DevPlane& ref, int 
   return (int)s;
 }
 
-// satd8_q: the 8x8 SATD of a cur block against the quarter-pel prediction at (qx, qy).
-__device__ __forceinline__ int satd8_q(const uint32_t* c, const DevPlane& ref, int x0, int y0, int qx, int qy) {
+// satd8_q: the 8x8 SATD of a cur block (its four tiles row-transformed, cc[tile][16]) against the
+// quarter-pel prediction at (qx, qy).
+__device__ __forceinline__ int satd8_q(const int (*cc)[16], const DevPlane& ref, int x0, int y0, int qx, int qy) {
   DevPlane ph = ref;
   ph.p = ref.p + (long long)((qy & 3) * 4 + (qx & 3)) * ref.phase;
   const int x = x0 + (qx >> 2), y = y0 + (qy >> 2);
@@ -94,14 +103,14 @@ __device__ __forceinline__ int satd8_q(const uint32_t* c, const DevPlane& ref, i
   for (int ty = 0; ty < 2; ty++)
 #pragma unroll
     for (int tx = 0; tx < 2; tx++) {
-      uint32_t ce[4], co[4], pr[4];
+      uint32_t pr[4];
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const uint32_t cw = c[2 * (4 * ty + i) + tx];
-        ce[i] = bytes_even(cw), co[i] = bytes_odd(cw);
+      for (int i = 0; i < 4; i++)
         pr[i] = in ? load4(p + (long long)(4 * ty + i) * ph.stride + 4 * tx) : row4(ph, x + 4 * tx, y + 4 * ty + i);
-      }
-      total += satd4_bytes(ce, co, pr);
+      int C[16];
+#pragma unroll
+      for (int k = 0; k < 16; k++) C[k] = cc[2 * ty + tx][k];
+      total += satd4_rows(C, pr);
     }
   return total;
 }
@@ -135,6 +144,13 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
   }
   if (tid == 0) S.nsearch = 0;
   __syncthreads();
+  if (level == 0)  // the refinement's cur tiles, row-transformed once per cell
+    for (int e = tid; e < kMeCells * 16; e += kMeThreads) {
+      const int c = e >> 4, t = (e >> 2) & 3, i = e & 3;
+      const uint32_t cw = S.cur[c][2 * (4 * (t >> 1) + i) + (t & 1)];
+#pragma unroll
+      for (int k = 0; k < 4; k++) S.ccoef[c][t][4 * k + i] = dp4a_us(cw, wh_row(k), 0);
+    }
   const bool top = level == kLevels - 1;
   if (!top && tid < kMeCells * 6) {
     const int c = tid / 6, k = tid - c * 6;
@@ -186,7 +202,9 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
   __syncthreads();
   const int nsearch = S.nsearch;
   // windows: rows y0 + cy - 8 .. + 23, 32 bytes from the 8-byte boundary at or below x0 + cx - 8;
-  // inside the margin as 8-byte loads, else word by word with clamping
+  // inside the margin as asynchronous 8-byte copies (all in flight at once: one memory latency for
+  // the whole staging), else word by word with clamping. Plane rows start 8-byte aligned (strides
+  // and margins are multiples of 8), and so do the window rows in shared memory.
   for (int e = tid; e < nsearch * kWinRows * 4; e += kMeThreads) {
     const int s = e / (kWinRows * 4), rem = e - s * (kWinRows * 4);
     const int rr = rem >> 2, qd = rem & 3;
@@ -194,12 +212,12 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
     const int wx = (bx * 8 + S.sx[s] - kMeRange) & ~7, wy = by * 8 + S.sy[s] - kMeRange;
     uint32_t* dst = S.win + s * kWinStride + rr * kWinWords + 2 * qd;
     if (inside(ref, wx, wy, 4 * kWinWords, kWinRows)) {
-      const uint2 v = __ldg(reinterpret_cast<const uint2*>(ref.p + (long long)(wy + rr) * ref.stride + wx + 8 * qd));
-      dst[0] = v.x, dst[1] = v.y;
+      cp_async8(dst, ref.p + (long long)(wy + rr) * ref.stride + wx + 8 * qd);
     } else {
       dst[0] = row4(ref, wx + 8 * qd, wy + rr), dst[1] = row4(ref, wx + 8 * qd + 4, wy + rr);
     }
   }
+  cp_async_wait_all();
   __syncthreads();
 
   // ---- C. +-8 search (me_search, inter_common.h:108-119): a thread per (search, dx) ----
@@ -254,7 +272,7 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
       for (int item = tid; item < ncells * 9; item += kMeThreads) {
         const int c = item / 9, t = item - c * 9, n = refine_pos(t);
         const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
-        S.rsatd[c][t] = satd8_q(S.cur[c], ref, bx * 8, by * 8, S.mvx[c] + (n % 3 - 1) * step, S.mvy[c] + (n / 3 - 1) * step);
+        S.rsatd[c][t] = satd8_q(S.ccoef[c], ref, bx * 8, by * 8, S.mvx[c] + (n % 3 - 1) * step, S.mvy[c] + (n / 3 - 1) * step);
       }
       __syncthreads();
       if (tid < ncells) {

@@ -15,6 +15,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import threading
+import weakref
 
 import numpy as np
 
@@ -54,6 +55,7 @@ SIGNATURES = {
     "celv2_reserve_group": (C.c_int, [C.c_void_p, C.c_int]),
     "celv2_group_records": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "celv2_clear_store": (C.c_int, [C.c_void_p]),
+    "celv2_drop_frame": (C.c_int, [C.c_void_p, C.c_longlong]),
     "celv2_debug_field": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int32), C.POINTER(C.c_int),
                                     C.POINTER(C.c_int)]),
     "celv2_debug_intra": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
@@ -70,6 +72,9 @@ SIGNATURES = {
                                      C.POINTER(C.POINTER(C.c_longlong)), C.POINTER(C.c_int64), C.c_int]),
     "celv2_set_config": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "celv2_get_config": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "celv2_set_output": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "celv2_host_alloc": (C.c_int, [C.c_longlong, C.POINTER(C.c_void_p)]),
+    "celv2_host_free": (C.c_int, [C.c_void_p]),
 }
 
 CFG_PERSISTENT, CFG_GRAPHS, CFG_PERSISTENT_OFF, CFG_INTER_CHUNK, CFG_ME_CELLS_L0 = 1, 2, 3, 4, 10
@@ -103,6 +108,48 @@ def _check(rc: int) -> None:
     if rc == E_INVAL:
         raise RuntimeError(msg)
     raise RuntimeError(f"CUDA engine error {rc}: {msg}")
+
+
+class _RecordPool:
+    """Page-locked record arrays (celv2_host_alloc) for the records the engine copies straight into
+    the caller's DecisionMap (celv2_set_output): no copy on the host, and the device-to-host copies
+    run as DMA. A buffer goes back to the pool when the last array viewing it is gone."""
+
+    def __init__(self):
+        self._free: dict[int, list[int]] = {}
+        self._lock = threading.Lock()
+        # free bytes kept for reuse: allocating and freeing page-locked memory is slow (and
+        # cudaFreeHost waits for the device), so a pipeline's maps should cycle through the pool
+        self.keep_bytes = int(os.environ.get("CELV2_RECORD_POOL_BYTES", 2 << 30))
+        self._kept = 0
+
+    def take(self, count: int):
+        """(records array of `count` celv2_sb_out, its address)."""
+        nbytes = count * SB_OUT_DTYPE.itemsize
+        with self._lock:
+            lst = self._free.get(nbytes)
+            ptr = lst.pop() if lst else None
+            if ptr is not None:
+                self._kept -= nbytes
+        if ptr is None:
+            p = C.c_void_p()
+            _check(library().celv2_host_alloc(nbytes, C.byref(p)))
+            ptr = p.value
+        buf = (C.c_uint8 * nbytes).from_address(ptr)
+        fin = weakref.finalize(buf, self._give, nbytes, ptr)
+        fin.atexit = False  # the process's exit releases page-locked memory anyway
+        return np.ctypeslib.as_array(buf).view(SB_OUT_DTYPE), ptr
+
+    def _give(self, nbytes: int, ptr: int) -> None:
+        with self._lock:
+            if self._kept + nbytes <= self.keep_bytes:
+                self._free.setdefault(nbytes, []).append(ptr)
+                self._kept += nbytes
+                return
+        library().celv2_host_free(ptr)
+
+
+_records = _RecordPool()
 
 
 def _plane_of(f):
@@ -193,6 +240,9 @@ class CudaEngine:
         _check(lib.celv2_geometry(h, C.byref(sc), C.byref(sr)))
         self.sb_cols, self.sb_rows = sc.value, sr.value
         self.row_hook = None  # called by collect before it publishes a row (tests only)
+        # record arrays queued copies still write into: held until the engine is idle, so their
+        # page-locked memory cannot go back to the pool while a copy targets it
+        self._inflight: list = []
 
     def close(self) -> None:
         if getattr(self, "_h", None):
@@ -222,9 +272,14 @@ class CudaEngine:
         rarr = (CelvFrame * max(1, len(refs)))(*[make_frame(r, self.width, self.height, keep) for r in refs])
         karr = (C.c_longlong * len(refs))(*ref_keys) if ref_keys else None
         lam = _lam.lambda_q8(qindex) if lambda_q8 is None else lambda_q8
-        _check(library().celv2_launch(self._h, C.byref(s), rarr, len(refs), lam, karr, src_key))
+        # the rows land in dm's own page-locked records (its contents are defined once collected)
+        records, ptr = _records.take(self.sb_cols * self.sb_rows)
+        lib = library()
+        _check(lib.celv2_set_output(self._h, 0, ptr))
+        self._inflight.append(records)
+        _check(lib.celv2_launch(self._h, C.byref(s), rarr, len(refs), lam, karr, src_key))
         dm.sb_size, dm.sb_cols, dm.sb_rows = self.sb_size, self.sb_cols, self.sb_rows
-        dm.records = np.zeros(self.sb_cols * self.sb_rows, dtype=SB_OUT_DTYPE)
+        dm.records = records
 
     def prepare(self, nxt, key: int) -> None:
         keep: list = []
@@ -240,8 +295,8 @@ class CudaEngine:
         return list(arr)
 
     def collect(self, dm: DecisionMap, gate: RowGate) -> None:
-        """Copies every row into dm as it arrives and publishes it on gate; on failure fails the
-        gate and raises. Returns with no work pending."""
+        """Publishes every row on gate as its records arrive in dm (the launch copies them straight
+        into dm.records); on failure fails the gate and raises. Returns with no work pending."""
         lib = library()
         try:
             for r in self.row_order():
@@ -249,14 +304,12 @@ class CudaEngine:
                     self.row_hook(r)
                 ptr = C.c_void_p()
                 _check(lib.celv2_wait_row(self._h, r, C.byref(ptr)))
-                n = self.sb_cols
-                src = np.ctypeslib.as_array((C.c_uint8 * (n * SB_OUT_DTYPE.itemsize)).from_address(ptr.value))
-                dm.records[r * n:(r + 1) * n] = src.view(SB_OUT_DTYPE)
                 gate.publish_one(r)
-            _check(lib.celv2_finish(self._h))
+            self.finish()
         except BaseException as e:
             gate.fail(e)
-            lib.celv2_finish(self._h)
+            if lib.celv2_finish(self._h) == E_OK:
+                self._inflight.clear()
             raise
 
     def decide_inter(self, src, refs, qindex: int, ref_keys=None) -> DecisionMap:
@@ -277,8 +330,22 @@ class CudaEngine:
     def reserve_group(self, frames: int) -> None:
         _check(library().celv2_reserve_group(self._h, frames))
 
-    def launch_group(self, src_keys, ref_keys, qindex, to_host: bool = False) -> None:
+    def launch_group(self, src_keys, ref_keys, qindex, to_host: bool = False, dms=None) -> None:
+        """One batch from the frame store (celv2_launch_group). With dms (one DecisionMap per job),
+        each job's records come straight into its map's page-locked records; they are defined once
+        the batch is finished (finish(), group_records())."""
         n = len(src_keys)
+        if dms is not None:
+            if len(dms) != n:
+                raise ValueError("launch_group: one DecisionMap per job")
+            to_host = True
+            lib = library()
+            for j, dm in enumerate(dms):
+                records, ptr = _records.take(self.sb_cols * self.sb_rows)
+                _check(lib.celv2_set_output(self._h, j, ptr))
+                self._inflight.append(records)
+                dm.sb_size, dm.sb_cols, dm.sb_rows = self.sb_size, self.sb_cols, self.sb_rows
+                dm.records = records
         qs = qindex if isinstance(qindex, (list, tuple)) else [qindex] * n
         sk = (C.c_longlong * n)(*src_keys)
         nr = (C.c_int * n)(*[len(r) for r in ref_keys])
@@ -296,9 +363,67 @@ class CudaEngine:
 
     def finish(self) -> None:
         _check(library().celv2_finish(self._h))
+        self._inflight.clear()
 
     def clear_store(self) -> None:
         _check(library().celv2_clear_store(self._h))
+        self._group_keys = set()
+
+    def set_output(self, job: int, ptr: int) -> None:
+        """celv2_set_output: the next launch copies job's records to `ptr` (page-locked memory)."""
+        _check(library().celv2_set_output(self._h, job, ptr))
+
+    def drop_frame(self, key: int) -> None:
+        _check(library().celv2_drop_frame(self._h, key))
+
+    _SRC_KEYS, _TMP_KEYS = 1 << 62, 1 << 61  # store keys of decide_group's sources / unkeyed references
+
+    def decide_group(self, srcs, refs, qindex, ref_keys=None, wait: bool = True) -> list[DecisionMap]:
+        """Frames decided together, one launch per stage: the leaves of a mini-GOP as the
+        reference's Pipeline::code_group (src/pipeline.cpp:328-384) holds them. Job i decides
+        srcs[i] against refs[i] (nearest first); ref_keys[i] (optional) are launch's ref_keys, so a
+        reference seen before under its key is not uploaded again. The maps equal separate launch /
+        collect calls' maps. Inputs are copied before it returns; with wait=False the records are
+        defined after finish()."""
+        n = len(srcs)
+        if len(refs) != n or (ref_keys is not None and len(ref_keys) != n):
+            raise ValueError("decide_group: one reference list (and key list) per source")
+        keyed = getattr(self, "_group_keys", set())
+        counter = getattr(self, "_group_counter", 0)
+        need, jobs_src, jobs_refs, tmp = set(), [], [], []
+        for i in range(n):
+            ks = []
+            for r, f in enumerate(refs[i]):
+                k = None if ref_keys is None or ref_keys[i] is None else int(ref_keys[i][r])
+                if k is None:
+                    counter += 1
+                    k = self._TMP_KEYS | counter
+                    self.upload(f, k)
+                    tmp.append(k)
+                elif k not in keyed:
+                    if k >= self._TMP_KEYS:
+                        raise ValueError("decide_group: reference keys must be below 2**61")
+                    self.upload(f, k)
+                    keyed.add(k)
+                need.add(k)
+                ks.append(k)
+            counter += 1
+            sk = self._SRC_KEYS | counter
+            self.upload(srcs[i], sk)
+            jobs_src.append(sk)
+            jobs_refs.append(ks)
+        for k in [k for k in keyed if k not in need]:  # keyed references this group does not use
+            self.drop_frame(k)
+            keyed.discard(k)
+        self._group_keys, self._group_counter = keyed, counter
+        dms = [DecisionMap() for _ in range(n)]
+        qs = qindex if isinstance(qindex, (list, tuple)) else [qindex] * n
+        self.launch_group(jobs_src, jobs_refs, qs, dms=dms)
+        for k in jobs_src + tmp:  # queued work still reads them; later uploads reuse the memory
+            self.drop_frame(k)
+        if wait:
+            self.finish()
+        return dms
 
     def set_config(self, key: int, value: int) -> None:
         _check(library().celv2_set_config(self._h, key, int(value)))
@@ -356,10 +481,24 @@ class CudaEngine:
         return out
 
 
-def launch_multi(jobs, qindex, to_host: bool = False) -> None:
+def launch_multi(jobs, qindex, to_host: bool = False, dms=None) -> None:
     """One batch over engines of different frame sizes: jobs = [(engine, src_key, [ref keys])].
-    Each engine's records come back with engine.group_records(k) for its k-th job here."""
+    Each engine's records come back with engine.group_records(k) for its k-th job here, or, with
+    dms (one DecisionMap per job), straight into the maps' records (defined once finished)."""
     n = len(jobs)
+    if dms is not None:
+        if len(dms) != n:
+            raise ValueError("launch_multi: one DecisionMap per job")
+        to_host = True
+        seen: dict = {}
+        for (e, _, _), dm in zip(jobs, dms):
+            k = seen.get(id(e), 0)
+            seen[id(e)] = k + 1
+            records, ptr = _records.take(e.sb_cols * e.sb_rows)
+            _check(library().celv2_set_output(e._h, k, ptr))
+            e._inflight.append(records)
+            dm.sb_size, dm.sb_cols, dm.sb_rows = e.sb_size, e.sb_cols, e.sb_rows
+            dm.records = records
     qs = qindex if isinstance(qindex, (list, tuple)) else [qindex] * n
     engs = (C.c_void_p * n)(*[e._h.value if isinstance(e._h, C.c_void_p) else e._h for e, _, _ in jobs])
     sk = (C.c_longlong * n)(*[s for _, s, _ in jobs])

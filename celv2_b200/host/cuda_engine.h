@@ -30,8 +30,26 @@ class CudaEngine : public DecisionEngine {
   void set_row_streams(int n) override;
   const std::string& device_name() const { return name_; }
 
+  // Several frames decided together, one kernel launch per stage for all of them: the leaves of a
+  // mini-GOP, which Pipeline::code_group (src/pipeline.cpp:328-384) otherwise hands to launch()
+  // one at a time. Frame i is srcs[i] against refs[i] (nearest first; keys[i] empty or one key per
+  // reference, as launch()'s ref_keys, so a reference seen before is not uploaded again) at
+  // qindex[i]; dms[i] is sized as launch() sizes it. The decisions equal separate launches'. The
+  // inputs are copied before it returns. At most 31 frames; collect_group must follow.
+  void launch_group(const std::vector<const Frame420*>& srcs, const std::vector<std::vector<const Frame420*>>& refs,
+                    const std::vector<std::vector<long long>>& keys, const std::vector<int>& qindex,
+                    std::vector<DecisionMap>& dms);
+  // Fills every dms[i] and publishes all of its rows on *gates[i], frame by frame; on failure
+  // fails every gate and rethrows. Returns with no work pending.
+  void collect_group(std::vector<DecisionMap>& dms, const std::vector<RowGate*>& gates);
+
  private:
   celv2_engine* e_ = nullptr;
   int width_, height_, sb_cols_ = 0, sb_rows_ = 0;
   std::string name_;
+  // launch_group's frame store: keyed references it uploaded, and a counter for the store keys of
+  // sources and unkeyed references (above the caller's key range)
+  std::vector<long long> keyed_;
+  long long next_key_ = 0;
+  int group_jobs_ = 0;
 };

@@ -89,7 +89,9 @@ const char* celv2_last_error(void);
 /* ---- Device-resident path (frames already in HBM; batching) ---- */
 
 /* Uploads a frame into the engine's keyed frame store (pyramid and quarter-pel phases), as a
- * reference would be; key >= 0. Later launches find it by key. */
+ * reference would be; key >= 0. Later launches find it by key (celv2_launch's ref_keys too). It
+ * stays until celv2_drop_frame / celv2_clear_store: celv2_launch's own cache of references does not
+ * evict it. The upload runs behind the queued work. */
 int celv2_upload(celv2_engine* e, const celv2_frame* f, long long key);
 
 /* One batch of frames decided from the frame store: job i decides the frame with key src_keys[i]
@@ -112,6 +114,20 @@ int celv2_group_records(celv2_engine* e, int job, const celv2_sb_out** records);
 
 /* Drops every frame of the store. */
 int celv2_clear_store(celv2_engine* e);
+/* Drops the stored frame with this key (none: nothing happens); a later upload reuses its device
+ * memory. Queued work that reads it still sees it: uploads run behind the queued work. */
+int celv2_drop_frame(celv2_engine* e, long long key);
+
+/* ---- Records straight into the caller's memory ----
+ * No counterpart in the reference, whose engines hand the records over through their own
+ * buffers. celv2_set_output names where the NEXT launch (celv2_launch: job 0; celv2_launch_group
+ * or celv2_launch_multi: this engine's job-th frame) copies its sb_cols * sb_rows records: page-
+ * locked host memory from celv2_host_alloc (any other memory: CELV2_EINVAL), or NULL for the
+ * engine's own buffer. It applies to that one launch; celv2_wait_row and celv2_group_records then
+ * return pointers into it. The caller keeps the memory until the launch is collected. */
+int celv2_set_output(celv2_engine* e, int job, celv2_sb_out* records);
+int celv2_host_alloc(long long bytes, void** out);
+int celv2_host_free(void* p);
 
 /* ---- A KEY-frame decision that allocates nothing ----
  * No counterpart in the reference. For callers that cannot allocate device memory while they run
@@ -144,8 +160,9 @@ long long celv2_kernel_launches(const celv2_engine* e);
  *  CELV2_CFG_PERSISTENT: 1 (default) -- each stage is one persistent kernel whose CTAs drain a
  *    device-side queue of the batch's work units (superblocks, cell groups); 0 -- one CTA per unit.
  *  CELV2_CFG_GRAPHS: 1 -- celv2_launch_group captures a batch's whole stage sequence (descriptor
- *    copy, queue reset, stage kernels, record copies) as a CUDA graph once per batch shape (the
- *    jobs' reference counts) and replays it; 0 (default) -- launches stage by stage.
+ *    copy, queue resets, stage kernels) as a CUDA graph once per batch shape (the jobs' reference
+ *    counts) and replays it, the record copies following it; 0 (default) -- launches stage by
+ *    stage.
  *  CELV2_CFG_PERSISTENT_OFF: a bit mask of stages that run one CTA per unit even when
  *    CELV2_CFG_PERSISTENT is on (bit l: motion-search level l, 5 intra, 6 inter, 7 finalize).
  *  CELV2_CFG_INTER_CHUNK: distinct MVs per pass of the inter stage, 8..64 (default 64).

@@ -244,6 +244,50 @@ static int errors_as_the_reference() {
   return 0;
 }
 
+// The leaves of a mini-GOP through launch_group / collect_group (what Pipeline::code_group,
+// src/pipeline.cpp:328-384, would call) against the CpuEngine deciding them one by one.
+static int group_matches_cpu_per_frame() {
+  const int w = 416, h = 240;
+  std::vector<Frame420> f;
+  for (int i = 0; i < 9; i++) f.push_back(scene_frame(w, h, 2 * i, -i, 3));
+  CudaEngine cuda(w, h, 64);
+  CpuEngine cpu(w, h, 64, 8);
+  // anchor and middle first (ordinary launches, keyed), then the leaves as one group
+  const std::vector<std::vector<int>> leaves_refs{{0, 2, 4}, {2, 4, 0}, {4, 6, 2}, {6, 8, 4}};
+  for (int pass = 0; pass < 2; pass++) {  // the second pass finds its keyed references stored
+    std::vector<const Frame420*> srcs;
+    std::vector<std::vector<const Frame420*>> refs;
+    std::vector<std::vector<long long>> keys;
+    for (size_t i = 0; i < leaves_refs.size(); i++) {
+      srcs.push_back(&f[2 * i + 1]);
+      refs.emplace_back();
+      keys.emplace_back();
+      for (int r : leaves_refs[i]) refs.back().push_back(&f[r]), keys.back().push_back(r);
+    }
+    std::vector<int> q{120, 90, 150, 120};
+    std::vector<DecisionMap> dms;
+    cuda.launch_group(srcs, refs, keys, q, dms);
+    std::vector<RowGate> gates(srcs.size());
+    std::vector<RowGate*> gp;
+    for (RowGate& g : gates) gp.push_back(&g);
+    cuda.collect_group(dms, gp);
+    for (size_t i = 0; i < srcs.size(); i++) {
+      CHECK_EQ(gates[i].ready_rows(), dms[i].sb_rows);
+      CHECK(identical(dms[i], run(cpu, *srcs[i], refs[i], q[i])));
+    }
+    // an ordinary launch in between, with a key the group path stored
+    CHECK(identical(run(cuda, f[3], {&f[2], &f[4]}, 120, {2, 4}), run(cpu, f[3], {&f[2], &f[4]}, 120)));
+  }
+  // without keys, and a KEY frame among inter frames
+  std::vector<DecisionMap> dms;
+  cuda.launch_group({&f[5], &f[7]}, {{}, {&f[6], &f[8]}}, {}, {120, 120}, dms);
+  std::vector<RowGate> gates(2);
+  cuda.collect_group(dms, {&gates[0], &gates[1]});
+  CHECK(identical(dms[0], run(cpu, f[5], {}, 120)));
+  CHECK(identical(dms[1], run(cpu, f[7], {&f[6], &f[8]}, 120)));
+  return 0;
+}
+
 int main() {
   int fails = 0;
   fails += RUN(cpu_engine_matches_cuda);
@@ -254,6 +298,7 @@ int main() {
   fails += RUN(rows_publish_before_collect_ends);
   fails += RUN(no_intra_block_wider_than_32);
   fails += RUN(errors_as_the_reference);
+  fails += RUN(group_matches_cpu_per_frame);
   if (fails) std::fprintf(stderr, "%d test(s) failed\n", fails);
   else std::printf("all adapter cases passed\n");
   return fails ? 1 : 0;

@@ -1,13 +1,15 @@
 """Batching changes the launch structure, not the decisions: persistent queue-draining stage
 kernels, CUDA-graph replay of a batch, and one batch over streams of different frame sizes must
 all give the oracle's records byte for byte."""
+import ctypes as C
 import json
 
+import numpy as np
 import pytest
 
 from celv2_b200 import lam, synth
 from celv2_b200 import engine as E
-from celv2_b200.records import first_difference, records_equal
+from celv2_b200.records import SB_OUT_DTYPE, DecisionMap, first_difference, records_equal
 
 pytestmark = pytest.mark.gpu
 
@@ -88,3 +90,67 @@ def test_autotuner_sets_a_valid_config(tmp_path, monkeypatch):
         assert [e.get_config(E.CFG_ME_CELLS_L0 + l) for l in range(5)] == chosen["me_cells"]
         again = tune.cached(e, "test-gpu", 7, [6, 5, 4, 3, 2, 1, 0])  # from the cache file
         assert again == json.loads(json.dumps(chosen))
+
+
+def test_records_land_in_caller_memory(oracle):
+    w, h = 416, 240
+    clip = synth.small_clip(seed=4, frames=3)
+    with E.CudaEngine(w, h) as e:
+        bad = np.zeros(e.sb_cols * e.sb_rows, dtype=SB_OUT_DTYPE)  # pageable memory is refused
+        with pytest.raises(RuntimeError):
+            e.set_output(0, bad.ctypes.data)
+        dm, gate = DecisionMap(), E.RowGate()
+        e.launch(clip[2].hy, [clip[1].hy, clip[0].hy], 120, dm)
+        e.collect(dm, gate)
+        ptr = C.c_void_p()
+        assert E.library().celv2_wait_row(e._h, 0, C.byref(ptr)) == 0
+        assert ptr.value == dm.records.ctypes.data  # the rows were copied into dm itself
+        check(oracle, w, h, clip, 2, [1, 0], 120, dm.records, "launch into caller memory")
+        keep = dm.records.copy()
+        dm2 = e.decide_inter(clip[1].hy, [clip[0].hy], 120)  # a later launch leaves dm alone
+        assert records_equal(dm.records, keep)
+        check(oracle, w, h, clip, 1, [0], 120, dm2.records, "second launch")
+
+
+@pytest.mark.parametrize("graphs", [0, 1])
+def test_decide_group_pipelined_matches_oracle(oracle, graphs):
+    """The mini-GOP through decide_group with every group in flight before the first is read:
+    double-buffered device records, copies overlapping the next group, keyed references reused."""
+    w, h = 416, 240
+    clip = synth.small_clip(seed=9, frames=9)
+    plan = [[(0, [])], [(8, [0])], [(4, [0, 8])], [(2, [0, 4, 8]), (6, [4, 8, 0])],
+            [(1, [0, 2, 4]), (3, [2, 4, 0]), (5, [4, 6, 2]), (7, [6, 8, 4])]]
+    with E.CudaEngine(w, h) as e:
+        e.set_config(E.CFG_GRAPHS, graphs)
+        for rep in range(2):
+            out = []
+            for group in plan:
+                dms = e.decide_group([clip[s].hy for s, _ in group], [[clip[r].hy for r in refs] for _, refs in group],
+                                     120, ref_keys=[list(refs) for _, refs in group], wait=False)
+                out.append(dms)
+            e.finish()
+            for group, dms in zip(plan, out):
+                for (s, refs), dm in zip(group, dms):
+                    check(oracle, w, h, clip, s, refs, 120, dm.records, f"rep {rep} frame {s}")
+
+
+def test_launch_multi_into_maps(oracle):
+    sizes = [(416, 240), (202, 122)]
+    clips = [synth.sinusoid_clip(w, h, 3, 50 + k, noise_sigma=3.0) for k, (w, h) in enumerate(sizes)]
+    engines = [E.CudaEngine(w, h) for w, h in sizes]
+    try:
+        for e, clip in zip(engines, clips):
+            for i, f in enumerate(clip):
+                e.upload(f.hy, i)
+        jobs = [(engines[0], 2, [1, 0]), (engines[1], 2, [1]), (engines[0], 1, [0])]
+        for rep in range(3):  # alternating device record buffers
+            dms = [DecisionMap() for _ in jobs]
+            E.launch_multi(jobs, 130, dms=dms)
+            for e in engines:
+                e.finish()
+            for (e, src, refs), dm in zip(jobs, dms):
+                i = engines.index(e)
+                check(oracle, *sizes[i], clips[i], src, refs, 130, dm.records, f"rep {rep} {sizes[i]} frame {src}")
+    finally:
+        for e in engines:
+            e.close()
