@@ -289,8 +289,8 @@ def stage_ops(counters, plan, steps):
     for l in range(5):
         centre = (cells[l] * steps * 6 * 64 * SAD_OPS) if l < 4 else 0
         search = counters[l] * 289 * 64 * SAD_OPS
-        refine = cells[0] * steps * 18 * 4 * H4_OPS if l == 0 else 0
-        ops[f"me_l{l}"] = float(centre + search + refine)
+        ops[f"me_l{l}"] = float(centre + search)
+    ops["me_refine"] = float(cells[0] * steps * 18 * 4 * H4_OPS)
     ops["intra"] = float(frames * steps * nsb * 2304 * 13 * H4_OPS)
     ops["inter"] = float(counters[5] * 256 * H4_OPS)
     ops["finalize"] = float(counters[6] * H4_OPS)
@@ -313,7 +313,8 @@ def stage_bytes(plan, steps):
     for l in range(5):
         w, h, c, r = level_dims(l)
         out[f"me_l{l}"] = float(steps * inter_refs * (2 * w * h + 3 * 4 * c * r))
-    w0, h0 = level_dims(0)[:2]
+    w0, h0, c0, r0 = level_dims(0)
+    out["me_refine"] = float(steps * inter_refs * (2 * w0 * h0 + 8 * c0 * r0))
     out["intra"] = float(steps * frames * (w0 * h0 + nsb * 425 * 13 * 4))
     out["inter"] = float(steps * inter_refs * (2 * w0 * h0 + nsb * 425 * 8))
     out["finalize"] = float(steps * (inter_refs * nsb * 425 * 8 + frames * nsb * (425 * 13 * 4 + RECORD_BYTES)))

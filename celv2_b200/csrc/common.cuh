@@ -95,7 +95,8 @@ __device__ __forceinline__ uint32_t load4(const uint8_t* p) {
   return __funnelshift_r(lo, __ldg(w + 1), sh);
 }
 
-// Sum of absolute 4x4 Hadamard coefficients (src/gpu/intra_common.h:131-146): rows, then columns.
+// Sum of absolute 4x4 Hadamard coefficients (src/gpu/intra_common.h:131-146): rows, then columns,
+// the last column butterfly folded with the absolute values: |x + y| + |x - y| = 2 max(|x|, |y|).
 __device__ __forceinline__ int hadamard4x4(int d[16]) {
 #pragma unroll
   for (int r = 0; r < 4; r++) {
@@ -108,9 +109,9 @@ __device__ __forceinline__ int hadamard4x4(int d[16]) {
   for (int c = 0; c < 4; c++) {
     const int s01 = d[c] + d[4 + c], d01 = d[c] - d[4 + c];
     const int s23 = d[8 + c] + d[12 + c], d23 = d[8 + c] - d[12 + c];
-    sum += abs(s01 + s23) + abs(d01 + d23) + abs(s01 - s23) + abs(d01 - d23);
+    sum += max(abs(s01), abs(s23)) + max(abs(d01), abs(d23));
   }
-  return sum;
+  return 2 * sum;
 }
 
 // Columns 0 and 2 (even) or 1 and 3 (odd) of a 4-byte row as two 16-bit lanes.

@@ -174,7 +174,8 @@ struct Stage {
 };
 
 // Stages timed by CUDA events when stage timing is on (celv2_stage_timing).
-enum StageId { kStUpload, kStPhases, kStMe4, kStMe3, kStMe2, kStMe1, kStMe0, kStIntra, kStInter, kStFinalize, kStages };
+enum StageId { kStUpload, kStPhases, kStMe4, kStMe3, kStMe2, kStMe1, kStMe0, kStIntra, kStInter, kStFinalize, kStRefine,
+               kStages };
 
 // Per-frame device buffers of a decision.
 struct JobBuffers {
@@ -244,7 +245,7 @@ struct celv2_engine {
   long long stage_n[kStages] = {};
   unsigned long long* stats = nullptr;  // device work counters (kStats), while timing
   // stage work queues (device counters): [0..4] motion search levels, [5] intra, [6] inter,
-  // [7] finalize of the main stream; [8] prepare's intra
+  // [7] finalize, [8] level 0's refinement of the main stream; [15] prepare's intra
   unsigned* queues = nullptr;
   bool persistent = true;      // the queue-draining persistent stage kernels (else one CTA per unit)
   unsigned persistent_off = 0; // stages (bit i: queue i) that run one CTA per unit anyway
@@ -514,7 +515,7 @@ struct celv2_engine {
   int enqueue_stages(const std::vector<FrameJob>& jobs, bool with_intra, cudaStream_t stream) {
     const int n = (int)jobs.size();
     int launched = 0;
-    if (persistent) CK(cudaMemsetAsync(queues, 0, 8 * sizeof(unsigned), stream));
+    if (persistent) CK(cudaMemsetAsync(queues, 0, 9 * sizeof(unsigned), stream));
     auto q = [&](int i) { return persistent && !(persistent_off >> i & 1) ? queues + i : nullptr; };
     WorkList w{};
     w.njobs = n;
@@ -526,6 +527,13 @@ struct celv2_engine {
         stage(kStMe0 - l, stream, [&] { launch_me_level(djobs, w, l, me_cells[l], stream); });
         launched++;
       }
+    }
+    for (int j = 0; j < n; j++)
+      w.prefix[j + 1] = w.prefix[j] + refine_units(jobs[j].nrefs, jobs[j].fcols[0], jobs[j].frows[0]);
+    w.queue = q(8);
+    if (w.prefix[n] > 0) {
+      stage(kStRefine, stream, [&] { launch_me_refine(djobs, w, stream); });
+      launched++;
     }
     if (with_intra) {
       for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].sb_cols * jobs[j].sb_rows;
@@ -649,8 +657,8 @@ struct celv2_engine {
     w.njobs = 1;
     w.prefix[1] = g.nsb;
     if (persistent) {
-      CK(cudaMemsetAsync(queues + 8, 0, sizeof(unsigned), prep_st));
-      w.queue = queues + 8;
+      CK(cudaMemsetAsync(queues + 15, 0, sizeof(unsigned), prep_st));
+      w.queue = queues + 15;
     }
     stage(kStIntra, prep_st, [&] { launch_intra(dprep, w, prep_st); });
     kernel_launches++;
@@ -1193,7 +1201,7 @@ int celv2_set_config(celv2_engine* e, int key, int value) {
     switch (key) {
       case CELV2_CFG_PERSISTENT: e->persistent = value != 0, e->free_graphs(); break;
       case CELV2_CFG_GRAPHS: e->use_graphs = value != 0; break;
-      case CELV2_CFG_PERSISTENT_OFF: e->persistent_off = (unsigned)value & 0xff, e->free_graphs(); break;
+      case CELV2_CFG_PERSISTENT_OFF: e->persistent_off = (unsigned)value & 0x1ff, e->free_graphs(); break;
       case CELV2_CFG_INTER_CHUNK:
         if (value < 8 || value > 64) invalid("inter chunk must be 8..64");
         e->inter_chunk = value, e->free_graphs();

@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(kFinThreads, 3) k_finalize(const FrameJob* __r
   const int2* inter = job.inter + (long long)sb * kMaxRefs * kBlocks;
 
   // 1. each reference's best, the best two references, the records per reference
+  unsigned comp_tiles = 0;  // work counter: compound 4x4 tiles
   for (int b = tid; b < kBlocks; b += kFinThreads) {
     long long rc[kMaxRefs];
     int rmv[kMaxRefs];
@@ -78,16 +79,20 @@ __global__ void __launch_bounds__(kFinThreads, 3) k_finalize(const FrameJob* __r
     S.inter_mv[b] = a >= 0 ? rmv[a] : 0;
     S.inter_ref[b] = a >= 0 ? a : 0;
     const bool comp = second >= 0 && compound_pair_ok(a, second, nrefs);
-    if (comp && job.stats) {
+    if (comp) {
       int bx, by, bw, bh;
       sb_block_geom(b, bx, by, bw, bh);
-      atomicAdd(job.stats + kStatCompoundTiles, (unsigned long long)(bw / 4) * (bh / 4));
+      comp_tiles += (unsigned)(bw / 4) * (bh / 4);
     }
     S.comp_a[b] = comp ? a : -1;
     S.comp_b[b] = comp ? second : 0;
     S.comp_mv0[b] = comp ? rmv[a] : 0;
     S.comp_mv1[b] = comp ? rmv[second] : 0;
     S.comp_sum[b] = 0;
+  }
+  if (job.stats) {  // one atomic per warp
+    comp_tiles = __reduce_add_sync(0xffffffffu, comp_tiles);
+    if ((tid & 31) == 0 && comp_tiles) atomicAdd(job.stats + kStatCompoundTiles, (unsigned long long)comp_tiles);
   }
   __syncthreads();
 

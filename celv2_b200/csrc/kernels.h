@@ -53,11 +53,14 @@ void launch_expand_u16(const uint16_t* raw, int pitch, int bit_depth, const DevP
 void launch_pyramid(const DevPyramid& pyr, cudaStream_t st);
 void launch_phases(const DevPlane& lv0, cudaStream_t st);
 
-// Motion search of one pyramid level for every (job, reference, 8x8 cell); level 0 includes the
-// quarter-pel refinement. Units: me_units(nrefs, fcols[level], frows[level], cells) per job (groups
+// Motion search of one pyramid level for every (job, reference, 8x8 cell), whole-pel (level 0's
+// field in quarter pels). Units: me_units(nrefs, fcols[level], frows[level], cells) per job (groups
 // of `cells` cells of one reference; cells 16 or 32).
 int me_units(int nrefs, int cols, int rows, int cells);
 void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, int cells, cudaStream_t st);
+// Level 0's quarter-pel refinement, in place. Units: refine_units(nrefs, fcols[0], frows[0]) per job.
+int refine_units(int nrefs, int cols, int rows);
+void launch_me_refine(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
 
 // Intra SATDs of every candidate block and mode. Units: sb_cols * sb_rows per job.
 void launch_intra(const FrameJob* jobs, const WorkList& w, cudaStream_t st);

@@ -16,9 +16,8 @@
 //     one of the 17 dy accumulators whose 8x8 block covers that row -- 24 row loads instead of
 //     17 x 8 per column. The column's best (cost << 9 | raster index) goes to a shared atomicMin,
 //     which yields the reference's first strict minimum in dy-major order;
-//  D. at level 0, the 9 positions of each refinement step are (cell, position) items computing the
-//     8x8 quarter-pel SATD from the phase planes; one thread per cell replays the centre-first
-//     strict choice.
+// Level 0's quarter-pel refinement is its own kernel (k_me_refine): one thread per (cell, position)
+// of each step, every CTA full, instead of a tail phase that leaves most of this one idle.
 // Integer ALU bound: 289 x 16 byte-SIMD absolute-difference accumulates per searched centre.
 #include "kernels.h"
 
@@ -34,14 +33,11 @@ template <int CELLS>
 struct MeSmem {
   static constexpr int kSearches = 2 * CELLS;  // at most two centres per cell
   uint32_t cur[CELLS][16];
-  int ccoef[CELLS][4][16];  // level 0: each 4x4 tile's row-transformed cur rows (satd4_rows)
   int csad[CELLS][6];
   int ccx[CELLS][6], ccy[CELLS][6];
   int scell[kSearches], sx[kSearches], sy[kSearches], soff[kSearches];
   unsigned skey[kSearches];
   int first_search[CELLS], two[CELLS];
-  int mvx[CELLS], mvy[CELLS];
-  int rsatd[CELLS][9];
   int nsearch;
   alignas(16) uint32_t win[kSearches * kWinStride];
 };
@@ -90,31 +86,6 @@ __device__ __forceinline__ int sad8(const uint32_t* c, const DevPlane& ref, int 
   return (int)s;
 }
 
-// satd8_q: the 8x8 SATD of a cur block (its four tiles row-transformed, cc[tile][16]) against the
-// quarter-pel prediction at (qx, qy).
-__device__ __forceinline__ int satd8_q(const int (*cc)[16], const DevPlane& ref, int x0, int y0, int qx, int qy) {
-  DevPlane ph = ref;
-  ph.p = ref.p + (long long)((qy & 3) * 4 + (qx & 3)) * ref.phase;
-  const int x = x0 + (qx >> 2), y = y0 + (qy >> 2);
-  const bool in = inside(ph, x, y, 8, 8);
-  const uint8_t* p = ph.p + (long long)y * ph.stride + x;
-  int total = 0;
-#pragma unroll
-  for (int ty = 0; ty < 2; ty++)
-#pragma unroll
-    for (int tx = 0; tx < 2; tx++) {
-      uint32_t pr[4];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-        pr[i] = in ? load4(p + (long long)(4 * ty + i) * ph.stride + 4 * tx) : row4(ph, x + 4 * tx, y + 4 * ty + i);
-      int C[16];
-#pragma unroll
-      for (int k = 0; k < 16; k++) C[k] = cc[2 * ty + tx][k];
-      total += satd4_rows(C, pr);
-    }
-  return total;
-}
-
 // The refinement step's position n (raster 0..8 with the centre, 4, visited first).
 __device__ __forceinline__ int refine_pos(int t) { return t == 0 ? 4 : (t <= 4 ? t - 1 : t); }
 
@@ -144,13 +115,6 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
   }
   if (tid == 0) S.nsearch = 0;
   __syncthreads();
-  if (level == 0)  // the refinement's cur tiles, row-transformed once per cell
-    for (int e = tid; e < kMeCells * 16; e += kMeThreads) {
-      const int c = e >> 4, t = (e >> 2) & 3, i = e & 3;
-      const uint32_t cw = S.cur[c][2 * (4 * (t >> 1) + i) + (t & 1)];
-#pragma unroll
-      for (int k = 0; k < 4; k++) S.ccoef[c][t][4 * k + i] = dp4a_us(cw, wh_row(k), 0);
-    }
   const bool top = level == kLevels - 1;
   if (!top && tid < kMeCells * 6) {
     const int c = tid / 6, k = tid - c * 6;
@@ -262,36 +226,101 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
       const unsigned k2 = S.skey[s0 + 1];
       if ((k2 >> 9) < (k1 >> 9)) mx = S.sx[s0 + 1] + (int)(k2 & 511) % 17 - kMeRange, my = S.sy[s0 + 1] + (int)(k2 & 511) / 17 - kMeRange;
     }
-    S.mvx[tid] = level == 0 ? mx * 4 : mx, S.mvy[tid] = level == 0 ? my * 4 : my;
+    // level 0 in quarter pels: k_me_refine refines it in place
+    job.field[r][level][cell0 + tid] = level == 0 ? pack_mv(mx * 4, my * 4) : pack_mv(mx, my);
   }
-  __syncthreads();
-
-  // ---- D. quarter-pel refinement at level 0 (me_refine, inter_common.h:141-154) ----
-  if (level == 0) {
-    for (int step = 2; step >= 1; step--) {
-      for (int item = tid; item < ncells * 9; item += kMeThreads) {
-        const int c = item / 9, t = item - c * 9, n = refine_pos(t);
-        const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
-        S.rsatd[c][t] = satd8_q(S.ccoef[c], ref, bx * 8, by * 8, S.mvx[c] + (n % 3 - 1) * step, S.mvy[c] + (n / 3 - 1) * step);
-      }
-      __syncthreads();
-      if (tid < ncells) {
-        const int cx = S.mvx[tid], cy = S.mvy[tid];
-        int best = S.rsatd[tid][0], nx = cx, ny = cy;
-        for (int t = 1; t < 9; t++) {
-          const int s = S.rsatd[tid][t] + kSubpelPenalty, n = refine_pos(t);
-          if (s < best) best = s, nx = cx + (n % 3 - 1) * step, ny = cy + (n / 3 - 1) * step;
-        }
-        S.mvx[tid] = nx, S.mvy[tid] = ny;
-      }
-      __syncthreads();
-    }
-  }
-  if (tid < ncells) {
-    job.field[r][level][cell0 + tid] = pack_mv(S.mvx[tid], S.mvy[tid]);
-    if (job.stats) atomicAdd(job.stats + level, S.two[tid] ? 2ull : 1ull);
+  if (job.stats && tid < 32) {  // searched centres, one atomic per unit (the cells sit in warp 0)
+    const unsigned n = __reduce_add_sync(0xffffffffu, tid < ncells ? (S.two[tid] ? 2u : 1u) : 0u);
+    if (tid == 0) atomicAdd(job.stats + level, (unsigned long long)n);
   }
   }  // units
+}
+
+// ---- quarter-pel refinement of level 0 (me_refine, inter_common.h:141-154) ----
+// One CTA per kRefineCells cells of one (job, reference); each step's 9 positions x 4 tiles are
+// (cell, position, tile) items -- one 4x4 quarter-pel SATD each from the phase planes, the cur
+// tiles row-transformed once per cell -- summed per position by shuffles (a position's four tiles
+// are four adjacent lanes); one thread per cell replays the centre-first strict choice. Small
+// items and few registers: many CTAs per SM to hide the loads' latency. (Its cost is the L1
+// traffic of rows scattered over nine phase planes; staging them in shared memory first did not
+// fetch fewer lines and added index arithmetic.)
+constexpr int kRefineCells = 7, kRefineThreads = 256;  // 7 x 36 = 252 items
+
+__global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
+  __shared__ int cc[kRefineCells][4][16];
+  __shared__ int sat[kRefineCells][9];
+  __shared__ int mvx[kRefineCells], mvy[kRefineCells];
+  __shared__ int unit_slot;
+  const int tid = threadIdx.x;
+  int unit, iter = 0;
+  while (take_unit(w, unit, iter, &unit_slot)) {
+  const int jb = job_of(w, unit);
+  const FrameJob& job = jobs[jb];
+  const int cols = job.fcols[0], ncell = cols * job.frows[0];
+  const int groups = (ncell + kRefineCells - 1) / kRefineCells;
+  const int u = unit - w.prefix[jb];
+  const int r = u / groups, cell0 = (u - r * groups) * kRefineCells;
+  const int ncells = min(kRefineCells, ncell - cell0);
+  const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
+  int* field = job.field[r][0];
+  if (tid < ncells * 16) {
+    const int c = tid >> 4, t = (tid >> 2) & 3, i = tid & 3;
+    const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
+    const uint32_t cw = row4(cur, bx * 8 + 4 * (t & 1), by * 8 + 4 * (t >> 1) + i);
+#pragma unroll
+    for (int k = 0; k < 4; k++) cc[c][t][4 * k + i] = dp4a_us(cw, wh_row(k), 0);
+  }
+  if (tid < ncells) {
+    const int m = field[cell0 + tid];
+    mvx[tid] = mv_x(m), mvy[tid] = mv_y(m);
+  }
+  __syncthreads();
+  // this thread's item (threads past the last item work on item 0 and drop the result)
+  const bool valid = tid < ncells * 36;
+  const int it = valid ? tid : 0, c = it / 36, rem = it - c * 36, t = rem >> 2, tile = rem & 3;
+  const int n = refine_pos(t), cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
+  const int x0 = bx * 8 + 4 * (tile & 1), y0 = by * 8 + 4 * (tile >> 1);
+  for (int step = 2; step >= 1; step--) {
+    const int qx = mvx[c] + (n % 3 - 1) * step, qy = mvy[c] + (n / 3 - 1) * step;
+    DevPlane ph = ref;
+    ph.p = ref.p + (long long)((qy & 3) * 4 + (qx & 3)) * ref.phase;
+    const int x = x0 + (qx >> 2), y = y0 + (qy >> 2);
+    uint32_t pr[4];
+    if (inside(ph, x, y, 4, 4)) {
+      const uint8_t* p = ph.p + (long long)y * ph.stride + x;
+#pragma unroll
+      for (int i = 0; i < 4; i++) pr[i] = load4(p + (long long)i * ph.stride);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; i++) pr[i] = row4(ph, x, y + i);
+    }
+    int v = satd4_rows(cc[c][tile], pr);  // the cur coefficients read from shared memory as used
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    if (valid && tile == 0) sat[c][t] = v;
+    __syncthreads();
+    if (tid < ncells) {
+      const int cx = mvx[tid], cy = mvy[tid];
+      int best = sat[tid][0], nx = cx, ny = cy;
+      for (int k = 1; k < 9; k++) {
+        const int s = sat[tid][k] + kSubpelPenalty, m = refine_pos(k);
+        if (s < best) best = s, nx = cx + (m % 3 - 1) * step, ny = cy + (m / 3 - 1) * step;
+      }
+      mvx[tid] = nx, mvy[tid] = ny;
+    }
+    __syncthreads();
+  }
+  if (tid < ncells) field[cell0 + tid] = pack_mv(mvx[tid], mvy[tid]);
+  }  // units
+}
+
+int refine_units(int nrefs, int cols, int rows) { return nrefs * ((cols * rows + kRefineCells - 1) / kRefineCells); }
+
+void launch_me_refine(const FrameJob* jobs, const WorkList& w, cudaStream_t st) {
+  const int units = w.prefix[w.njobs];
+  if (units <= 0) return;
+  const int grid = w.queue ? persistent_grid((const void*)k_me_refine, kRefineThreads, 0, units) : units;
+  k_me_refine<<<grid, kRefineThreads, 0, st>>>(jobs, w);
 }
 
 int me_units(int nrefs, int cols, int rows, int cells) { return nrefs * ((cols * rows + cells - 1) / cells); }
@@ -321,8 +350,10 @@ static cudaError_t attributes_cells() {
 }
 
 cudaError_t me_attributes() {
-  const cudaError_t e = attributes_cells<16>();
-  return e != cudaSuccess ? e : attributes_cells<32>();
+  cudaError_t e = attributes_cells<16>();
+  if (e == cudaSuccess) e = attributes_cells<32>();
+  if (e == cudaSuccess) persistent_grid((const void*)k_me_refine, kRefineThreads, 0, 1);  // fills the grid cache
+  return e;
 }
 
 }  // namespace celv2cu

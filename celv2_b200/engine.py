@@ -80,7 +80,7 @@ SIGNATURES = {
 CFG_PERSISTENT, CFG_GRAPHS, CFG_PERSISTENT_OFF, CFG_INTER_CHUNK, CFG_ME_CELLS_L0 = 1, 2, 3, 4, 10
 
 STAGE_NAMES = ["upload+pyramid", "phases", "me_l4", "me_l3", "me_l2", "me_l1", "me_l0", "intra", "inter",
-               "finalize"]
+               "finalize", "me_refine"]
 
 
 def library():

@@ -39,7 +39,7 @@ def autotune(eng: E.CudaEngine, src_key: int, ref_keys, qindex: int = 130, reps:
         for cells, persistent, chunk in itertools.product((16, 32), (0, 1), (32, 64)):
             for l in range(5):
                 eng.set_config(E.CFG_ME_CELLS_L0 + l, cells)
-            eng.set_config(E.CFG_PERSISTENT_OFF, 0 if persistent else 0xFF)
+            eng.set_config(E.CFG_PERSISTENT_OFF, 0 if persistent else 0x1FF)
             eng.set_config(E.CFG_INTER_CHUNK, chunk)
             results.append(((cells, persistent, chunk), _measure(eng, src_key, ref_keys, qindex, reps)))
     finally:
@@ -56,13 +56,13 @@ def autotune(eng: E.CudaEngine, src_key: int, ref_keys, qindex: int = 130, reps:
         chosen["me_cells"].append(cells)
         if not persistent:
             chosen["persistent_off"] |= 1 << l
-    for bit, stage in ((5, "intra"), (6, "inter"), (7, "finalize")):
+    for bit, stage in ((5, "intra"), (6, "inter"), (7, "finalize"), (8, "me_refine")):
         b = best(stage, None)
         if b and not b[1]:
             chosen["persistent_off"] |= 1 << bit
         if stage == "inter" and b:
             chosen["inter_chunk"] = b[2]
-    for stage in STAGES_ME + ["intra", "inter", "finalize"]:
+    for stage in STAGES_ME + ["me_refine", "intra", "inter", "finalize"]:
         chosen["stage_ms"][stage] = min(r[1][stage][0] for r in results) / reps
     apply(eng, chosen)
     return chosen

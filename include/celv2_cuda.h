@@ -164,7 +164,8 @@ long long celv2_kernel_launches(const celv2_engine* e);
  *    counts) and replays it, the record copies following it; 0 (default) -- launches stage by
  *    stage.
  *  CELV2_CFG_PERSISTENT_OFF: a bit mask of stages that run one CTA per unit even when
- *    CELV2_CFG_PERSISTENT is on (bit l: motion-search level l, 5 intra, 6 inter, 7 finalize).
+ *    CELV2_CFG_PERSISTENT is on (bit l: motion-search level l, 5 intra, 6 inter, 7 finalize,
+ *    8 level 0's quarter-pel refinement).
  *  CELV2_CFG_INTER_CHUNK: distinct MVs per pass of the inter stage, 8..64 (default 64).
  *  CELV2_CFG_ME_CELLS_L0 + l: 8x8 cells per motion-search CTA at pyramid level l, 16 or 32
  *    (default 32).
@@ -186,8 +187,8 @@ int celv2_stream(const celv2_engine* e, void** stream);
 /* Stage timing: when enabled, every stage launch is bracketed by CUDA events on its stream.
  * celv2_stage_times returns (and resets) the summed milliseconds and launch counts per stage, in
  * the order: uploads (8-bit level 0 + pyramid), quarter-pel phases, motion search levels 4, 3, 2,
- * 1, 0, intra, inter, finalize (CELV2_STAGES entries). */
-#define CELV2_STAGES 10
+ * 1, 0, intra, inter, finalize, level 0's quarter-pel refinement (CELV2_STAGES entries). */
+#define CELV2_STAGES 11
 int celv2_stage_timing(celv2_engine* e, int enable);
 int celv2_stage_times(celv2_engine* e, double* ms, long long* launches, int n);
 /* Work the kernels executed while stage timing was on, then reset: [l] motion-search centres
