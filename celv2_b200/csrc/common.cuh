@@ -58,11 +58,37 @@ struct FrameJob {
   // Work counters for the roofline (null unless stage timing is on): [l] searched centres at
   // level l, [5] distinct MVs summed over (superblock, reference), [6] compound 4x4 tiles.
   unsigned long long* stats;
+  // Pruning (null: the exhaustive search): per superblock, bit r keeps reference r, bit 7 keeps
+  // the intra modes (see keep_mask). The kept options are scored exactly as without pruning.
+  const uint8_t* keep;
+  long long* sb_cost;      // [sb]: the chosen partition's cost (null: not written)
 };
 
 enum { kStatInterMvs = 5, kStatCompoundTiles = 6, kStats = 8 };
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+// The effective keep mask of superblock sb: all options without pruning; otherwise the given
+// references (all of them if none is given in an inter frame) and, in inter frames, the intra
+// modes if bit 7 is set (a KEY frame always scores intra).
+__device__ __forceinline__ unsigned keep_mask(const FrameJob& job, int sb) {
+  const unsigned all = (1u << job.nrefs) - 1u;
+  if (!job.keep || job.nrefs == 0) return all | 0x80u;
+  const unsigned k = job.keep[sb];
+  return ((k & all) ? (k & all) : all) | (k & 0x80u);
+}
+
+// Whether level-0 cell (cx, cy) of reference r is read by the inter stage of a superblock that
+// keeps r: superblock (sx, sy) reads the cells sx * 8 - 1 .. sx * 8 + 8 (clamped), likewise in y.
+__device__ __forceinline__ bool cell_needed(const FrameJob& job, int r, int cx, int cy) {
+  if (!job.keep) return true;
+  const int x0 = cx >= 8 ? (cx - 1) >> 3 : 0, x1 = min(job.sb_cols - 1, (cx + 1) >> 3);
+  const int y0 = cy >= 8 ? (cy - 1) >> 3 : 0, y1 = min(job.sb_rows - 1, (cy + 1) >> 3);
+  for (int sy = y0; sy <= y1; sy++)
+    for (int sx = x0; sx <= x1; sx++)
+      if (keep_mask(job, sy * job.sb_cols + sx) >> r & 1u) return true;
+  return false;
+}
 
 // The clamped sample (Plane::at, src/gpu/intra_common.h:17-21).
 __device__ __forceinline__ int at(const DevPlane& s, int y, int x) {

@@ -184,6 +184,8 @@ struct JobBuffers {
   int2* inter = nullptr;     // nsb * kMaxRefs * kBlocks
   celv2_sb_out* out = nullptr;
   celv2_sb_out* out2 = nullptr;  // group buffers: the records of every other group (see group_parity)
+  uint8_t* keep = nullptr;       // pruning masks of the job, when given (nsb)
+  long long* sb_cost = nullptr;  // per superblock, the chosen partition's cost (nsb)
 };
 
 }  // namespace
@@ -197,6 +199,7 @@ struct celv2_engine {
   Slot srcs[2];                  // sources of launch / prepare
   int cur_src = 0;
   long long launches = 0;
+  long long launches_group = -1;  // the value of `launches` after the last group launch
   std::vector<Stage> stages;
   int next_stage = 0;
   JobBuffers single;             // the launch() path
@@ -205,6 +208,7 @@ struct celv2_engine {
   // caller memory for the next launch's records (celv2_set_output), per job; where the last
   // launch's records went (launch: last_out; group: group_out[job])
   celv2_sb_out* next_out[kMaxJobs] = {};
+  std::vector<uint8_t> next_keep[kMaxJobs];  // pruning masks for the next launch's jobs (celv2_set_keep)
   celv2_sb_out* last_out = nullptr;
   celv2_sb_out* group_out[kMaxJobs] = {};
   std::vector<cudaEvent_t> row_done;
@@ -331,6 +335,7 @@ struct celv2_engine {
 
   static void free_buffers(JobBuffers& b) {
     cudaFree(b.fields), cudaFree(b.intra), cudaFree(b.inter), cudaFree(b.out), cudaFree(b.out2);
+    cudaFree(b.keep), cudaFree(b.sb_cost);
     b = JobBuffers{};
   }
 
@@ -340,6 +345,8 @@ struct celv2_engine {
     CK(cudaMalloc(&b.inter, (size_t)g.nsb * kMaxRefs * kBlocks * sizeof(int2)));
     CK(cudaMalloc(&b.out, (size_t)g.nsb * sizeof(celv2_sb_out)));
     if (with_intra) CK(cudaMalloc(&b.out2, (size_t)g.nsb * sizeof(celv2_sb_out)));
+    CK(cudaMalloc(&b.keep, (size_t)g.nsb));
+    CK(cudaMalloc(&b.sb_cost, (size_t)g.nsb * sizeof(long long)));
   }
 
   void init(int width, int height, int dev) {
@@ -496,6 +503,25 @@ struct celv2_engine {
     job.out = b.out;
     job.lam = lam;
     job.stats = timing ? stats : nullptr;
+    job.sb_cost = b.sb_cost;
+  }
+
+  // The pruning masks named for the next launch's jobs (celv2_set_keep); clears them.
+  std::array<std::vector<uint8_t>, kMaxJobs> take_keeps() {
+    std::array<std::vector<uint8_t>, kMaxJobs> k;
+    for (int j = 0; j < kMaxJobs; j++) k[j].swap(next_keep[j]);
+    return k;
+  }
+
+  // A job's masks copied into b.keep on `stream` through the staging ring; null when none.
+  const uint8_t* put_keep(const std::vector<uint8_t>& k, const JobBuffers& b, cudaStream_t stream) {
+    if (k.empty()) return nullptr;
+    Stage& sg = take_stage(g.nsb);
+    std::memcpy(sg.host, k.data(), g.nsb);
+    CK(cudaMemcpyAsync(b.keep, sg.host, g.nsb, cudaMemcpyHostToDevice, stream));
+    CK(cudaEventRecord(sg.done, stream));
+    sg.pending = true;
+    return b.keep;
   }
 
   // Queues the copy of n descriptors to dst (device) through the pinned ring.
@@ -576,6 +602,7 @@ struct celv2_engine {
               long long src_key) {
     celv2_sb_out* dest = take_outputs()[0];  // this launch's, even when it fails
     if (!dest) dest = host_out;
+    const std::vector<uint8_t> keep0 = std::move(take_keeps()[0]);
     check_frame(src, "source");
     if (nrefs < 0 || nrefs > kMaxRefs) invalid("CudaEngine: too many references");
     for (int r = 0; r < nrefs; r++) check_frame(&refs[r], "reference");
@@ -614,6 +641,7 @@ struct celv2_engine {
       }
       std::vector<FrameJob> jobs(1);
       fill_job(jobs[0], srcs[use].pyr, used, nrefs, single, intra_prep[use], lam);
+      jobs[0].keep = put_keep(keep0, single, st);
       run_stages(jobs, !prepared, st);
       mark_used(used, nrefs, st);
       last_nrefs = nrefs;
@@ -760,6 +788,7 @@ struct celv2_engine {
   void launch_group(int njobs, const long long* src_keys, const int* nrefs, const long long* const* ref_keys,
                     const int64_t* lams, bool to_host) {
     const std::array<celv2_sb_out*, kMaxJobs> dests = take_outputs();
+    const std::array<std::vector<uint8_t>, kMaxJobs> keeps = take_keeps();
     if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per group");
     if (njobs > group_cap) reserve_group(std::max(njobs, 8));
     std::vector<FrameJob> jobs(njobs);
@@ -783,6 +812,7 @@ struct celv2_engine {
       }
       fill_job(jobs[j], cur->pyr, refs, nrefs[j], group[j], group[j].intra, lams[j]);
     }
+    for (int j = 0; j < njobs; j++) jobs[j].keep = put_keep(keeps[j], group[j], st);
     const int par = take_parity(st);
     for (int j = 0; j < njobs; j++) jobs[j].out = par ? group[j].out2 : group[j].out;
     if (use_graphs && !timing)
@@ -804,6 +834,7 @@ struct celv2_engine {
     }
     group_jobs = njobs;
     ++launches;
+    launches_group = launches;
     pending = true;
   }
 
@@ -878,7 +909,8 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     if (engines[j] && std::find(uniq.begin(), uniq.end(), engines[j]) == uniq.end()) uniq.push_back(engines[j]);
   // the caller memory named for this launch, which takes it even when it fails
   std::vector<std::array<celv2_sb_out*, kMaxJobs>> dests;
-  for (celv2_engine* e : uniq) dests.push_back(e->take_outputs());
+  std::vector<std::array<std::vector<uint8_t>, kMaxJobs>> keeps;
+  for (celv2_engine* e : uniq) dests.push_back(e->take_outputs()), keeps.push_back(e->take_keeps());
   if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per batch");
   for (int j = 0; j < njobs; j++) {
     if (!engines[j]) invalid("null engine");
@@ -932,6 +964,7 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     }
     Entry en;
     e->fill_job(en.job, cur->pyr, refs, nrefs[j], e->group[slot], e->group[slot].intra, lams[j]);
+    en.job.keep = e->put_keep(keeps[ei][slot], e->group[slot], lead->st);
     en.job.out = par[ei] ? e->group[slot].out2 : e->group[slot].out;
     en.e = e, en.slot = slot, en.work = (long long)(nrefs[j] + 1) * e->g.nsb, en.dest = dests[ei][slot];
     entries.push_back(en);
@@ -968,6 +1001,7 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     if (e != lead) CK(cudaStreamWaitEvent(e->st, done, 0));
     e->group_jobs = next[i];
     ++e->launches;
+    e->launches_group = e->launches;
     e->pending = true;
   }
   cudaEventDestroy(done);
@@ -1015,7 +1049,7 @@ int celv2_launch(celv2_engine* e, const celv2_frame* src, const celv2_frame* ref
   return guarded([&] {
     if (!e) invalid("null engine");
     if (nrefs > 0 && !refs) {
-      e->take_outputs();
+      e->take_outputs(), e->take_keeps();
       invalid("null references");
     }
     CK(cudaSetDevice(e->device));
@@ -1084,7 +1118,7 @@ int celv2_launch_group(celv2_engine* e, int njobs, const long long* src_keys, co
   return guarded([&] {
     if (!e) invalid("null engine");
     if (!src_keys || !nrefs || !lambda_q8) {
-      e->take_outputs();  // named for this launch, which fails
+      e->take_outputs(), e->take_keeps();  // named for this launch, which fails
       invalid("null argument");
     }
     CK(cudaSetDevice(e->device));
@@ -1108,6 +1142,29 @@ int celv2_group_records(celv2_engine* e, int job, const celv2_sb_out** records) 
     CK(cudaSetDevice(e->device));
     e->wait_idle();
     *records = e->group_out[job];
+  });
+}
+
+int celv2_set_keep(celv2_engine* e, int job, const uint8_t* keep) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    if (job < 0 || job >= kMaxJobs - 1) invalid("set_keep: job out of range");
+    if (keep)
+      e->next_keep[job].assign(keep, keep + e->g.nsb);
+    else
+      e->next_keep[job].clear();
+  });
+}
+
+int celv2_sb_costs(celv2_engine* e, int job, int64_t* out) {
+  return guarded([&] {
+    if (!e || !out) invalid("null argument");
+    const bool group = e->group_jobs > 0 && e->launches_group == e->launches;
+    if (job < 0 || (group ? job >= e->group_jobs : job != 0)) invalid("sb_costs: no such job in the last launch");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    const long long* src = group ? e->group[job].sb_cost : e->single.sb_cost;
+    CK(cudaMemcpy(out, src, (size_t)e->g.nsb * sizeof(long long), cudaMemcpyDeviceToHost));
   });
 }
 

@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(kFinThreads, 3) k_finalize(const FrameJob* __r
   const long long lam = job.lam;
   celv2_sb_out* o = job.out + sb;
   const int2* inter = job.inter + (long long)sb * kMaxRefs * kBlocks;
+  const unsigned keep = keep_mask(job, sb);  // pruned references and intra are not candidates
 
   // 1. each reference's best, the best two references, the records per reference
   unsigned comp_tiles = 0;  // work counter: compound 4x4 tiles
@@ -60,16 +61,20 @@ __global__ void __launch_bounds__(kFinThreads, 3) k_finalize(const FrameJob* __r
     int rmv[kMaxRefs];
     int a = -1, second = -1;
     for (int r = 0; r < nrefs; r++) {
+      if (!(keep >> r & 1u)) {
+        rc[r] = kMax, rmv[r] = 0;
+        continue;
+      }
       const int2 v = inter[r * kBlocks + b];
       rc[r] = (long long)v.x * 256 + lam * (kInterBits + r);
       rmv[r] = v.y;
       if (a < 0 || rc[r] < rc[a]) a = r;
     }
     for (int r = 0; r < nrefs; r++)
-      if (r != a && (second < 0 || rc[r] < rc[second])) second = r;
+      if (r != a && (keep >> r & 1u) && (second < 0 || rc[r] < rc[second])) second = r;
 #pragma unroll
     for (int r = 0; r < kMaxRefs; r++) {
-      const bool has = r < nrefs;
+      const bool has = r < nrefs && (keep >> r & 1u);
       const long long c8 = has ? rc[r] >> 8 : 0;
       o->c_rcost[r][b] = has ? (unsigned)(c8 < 0xfffffffeLL ? c8 : 0xfffffffeLL) : CELV2_NO_REF_COST;
       o->c_rmvx[r][b] = (short)(has ? mv_x(rmv[r]) : 0);
@@ -153,7 +158,7 @@ __global__ void __launch_bounds__(kFinThreads, 3) k_finalize(const FrameJob* __r
     }
     long long c = kMax;
     int m = 0;
-    if (b >= 5)
+    if (b >= 5 && (keep & 0x80u))
       for (int k = 0; k < kModes; k++) {
         const long long ck = (long long)intra[b * kModes + k] * 256 + lam * (mode_bits(k) + (nrefs > 0 ? kIntraInInterBits : 0));
         if (ck < c) c = ck, m = k;
@@ -199,6 +204,7 @@ __global__ void __launch_bounds__(kFinThreads, 3) k_finalize(const FrameJob* __r
     }
     __syncthreads();
   }
+  if (tid == 0 && job.sb_cost) job.sb_cost[sb] = S.sq_cost[0];
 
   // 5. the preorder tree and its leaves
   if (tid == 0) {

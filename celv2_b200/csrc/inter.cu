@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   const int nsb = job.sb_cols * job.sb_rows;
   const int u = unit - w.prefix[jb];
   const int r = u / nsb, sb = u - r * nsb, sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
+  if (!(keep_mask(job, sb) >> r & 1u)) continue;  // a pruned (superblock, reference): not scored
   const int ox = sbx * 64, oy = sby * 64;
   const int cols = job.fcols[0], rows = job.frows[0];
   const int* field = job.field[r][0];

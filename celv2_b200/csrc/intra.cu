@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(kIntraThreads, 3) k_intra(const FrameJob* __re
   const int jb = job_of(w, unit);
   const FrameJob& job = jobs[jb];
   const int sb = unit - w.prefix[jb], sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
+  if (!(keep_mask(job, sb) & 0x80u)) continue;  // intra pruned for this superblock
   const int ox = sbx * 64, oy = sby * 64;
   const DevPlane src = job.cur.lv[0];
 

@@ -38,6 +38,7 @@ struct MeSmem {
   int scell[kSearches], sx[kSearches], sy[kSearches], soff[kSearches];
   unsigned skey[kSearches];
   int first_search[CELLS], two[CELLS];
+  int need[CELLS];  // the cell is searched (level 0 of a pruned job: some superblock reads it)
   int nsearch;
   alignas(16) uint32_t win[kSearches * kWinStride];
 };
@@ -113,12 +114,16 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
     const int cell = cell0 + (c < ncells ? c : 0), by = cell / cols, bx = cell - by * cols;
     S.cur[c][k] = row4(cur, bx * 8 + 4 * (k & 1), by * 8 + (k >> 1));
   }
+  if (tid < kMeCells) {
+    const int cell = cell0 + tid, by = cell / cols, bx = cell - by * cols;
+    S.need[tid] = tid < ncells && (level != 0 || cell_needed(job, r, bx, by));
+  }
   if (tid == 0) S.nsearch = 0;
   __syncthreads();
   const bool top = level == kLevels - 1;
   if (!top && tid < kMeCells * 6) {
     const int c = tid / 6, k = tid - c * 6;
-    if (c < ncells) {
+    if (c < ncells && S.need[c]) {
       const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
       int cx = 0, cy = 0;  // k == 5: zero
       if (k < 5) {
@@ -135,7 +140,8 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
   __syncthreads();
 
   // ---- B. the two best distinct centres per cell, the search list ----
-  if (tid < ncells) {
+  if (tid < ncells && !S.need[tid]) S.first_search[tid] = -1, S.two[tid] = 0;
+  if (tid < ncells && S.need[tid]) {
     const int c = tid;
     int px = 0, py = 0, px2 = 0, py2 = 0;
     bool two = false;
@@ -218,7 +224,7 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
     atomicMin(&S.skey[s], best);
   }
   __syncthreads();
-  if (tid < ncells) {
+  if (tid < ncells && S.need[tid]) {
     const int s0 = S.first_search[tid];
     const unsigned k1 = S.skey[s0];
     int mx = S.sx[s0] + (int)(k1 & 511) % 17 - kMeRange, my = S.sy[s0] + (int)(k1 & 511) / 17 - kMeRange;
@@ -230,7 +236,7 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
     job.field[r][level][cell0 + tid] = level == 0 ? pack_mv(mx * 4, my * 4) : pack_mv(mx, my);
   }
   if (job.stats && tid < 32) {  // searched centres, one atomic per unit (the cells sit in warp 0)
-    const unsigned n = __reduce_add_sync(0xffffffffu, tid < ncells ? (S.two[tid] ? 2u : 1u) : 0u);
+    const unsigned n = __reduce_add_sync(0xffffffffu, tid < ncells && S.need[tid] ? (S.two[tid] ? 2u : 1u) : 0u);
     if (tid == 0) atomicAdd(job.stats + level, (unsigned long long)n);
   }
   }  // units
@@ -249,7 +255,7 @@ constexpr int kRefineCells = 7, kRefineThreads = 256;  // 7 x 36 = 252 items
 __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
   __shared__ int cc[kRefineCells][4][16];
   __shared__ int sat[kRefineCells][9];
-  __shared__ int mvx[kRefineCells], mvy[kRefineCells];
+  __shared__ int mvx[kRefineCells], mvy[kRefineCells], need[kRefineCells];
   __shared__ int unit_slot;
   const int tid = threadIdx.x;
   int unit, iter = 0;
@@ -272,11 +278,14 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob*
   }
   if (tid < ncells) {
     const int m = field[cell0 + tid];
+    const int cell = cell0 + tid, by = cell / cols, bx = cell - by * cols;
     mvx[tid] = mv_x(m), mvy[tid] = mv_y(m);
+    need[tid] = cell_needed(job, r, bx, by);
   }
   __syncthreads();
-  // this thread's item (threads past the last item work on item 0 and drop the result)
-  const bool valid = tid < ncells * 36;
+  // this thread's item (threads past the last item, or of a cell no superblock reads, work on item
+  // 0 and drop the result)
+  const bool valid = tid < ncells * 36 && need[tid / 36];
   const int it = valid ? tid : 0, c = it / 36, rem = it - c * 36, t = rem >> 2, tile = rem & 3;
   const int n = refine_pos(t), cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
   const int x0 = bx * 8 + 4 * (tile & 1), y0 = by * 8 + 4 * (tile >> 1);
@@ -299,7 +308,7 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob*
     v += __shfl_xor_sync(0xffffffffu, v, 2);
     if (valid && tile == 0) sat[c][t] = v;
     __syncthreads();
-    if (tid < ncells) {
+    if (tid < ncells && need[tid]) {
       const int cx = mvx[tid], cy = mvy[tid];
       int best = sat[tid][0], nx = cx, ny = cy;
       for (int k = 1; k < 9; k++) {
@@ -310,7 +319,7 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob*
     }
     __syncthreads();
   }
-  if (tid < ncells) field[cell0 + tid] = pack_mv(mvx[tid], mvy[tid]);
+  if (tid < ncells && need[tid]) field[cell0 + tid] = pack_mv(mvx[tid], mvy[tid]);
   }  // units
 }
 

@@ -75,6 +75,8 @@ SIGNATURES = {
     "celv2_set_output": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "celv2_host_alloc": (C.c_int, [C.c_longlong, C.POINTER(C.c_void_p)]),
     "celv2_host_free": (C.c_int, [C.c_void_p]),
+    "celv2_set_keep": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "celv2_sb_costs": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
 }
 
 CFG_PERSISTENT, CFG_GRAPHS, CFG_PERSISTENT_OFF, CFG_INTER_CHUNK, CFG_ME_CELLS_L0 = 1, 2, 3, 4, 10
@@ -372,6 +374,23 @@ class CudaEngine:
     def set_output(self, job: int, ptr: int) -> None:
         """celv2_set_output: the next launch copies job's records to `ptr` (page-locked memory)."""
         _check(library().celv2_set_output(self._h, job, ptr))
+
+    def set_keep(self, job: int, keep) -> None:
+        """celv2_set_keep: pruning masks (one byte per superblock) for job of the next launch;
+        None: the exhaustive search."""
+        if keep is None:
+            _check(library().celv2_set_keep(self._h, job, None))
+            return
+        k = np.ascontiguousarray(keep, dtype=np.uint8)
+        if k.size != self.sb_cols * self.sb_rows:
+            raise ValueError("set_keep: one byte per superblock")
+        _check(library().celv2_set_keep(self._h, job, k.ctypes.data))
+
+    def sb_costs(self, job: int = 0) -> np.ndarray:
+        """The last launch's per-superblock cost of the chosen partition (int64), job's."""
+        out = np.empty(self.sb_cols * self.sb_rows, dtype=np.int64)
+        _check(library().celv2_sb_costs(self._h, job, out.ctypes.data_as(C.POINTER(C.c_int64))))
+        return out
 
     def drop_frame(self, key: int) -> None:
         _check(library().celv2_drop_frame(self._h, key))

@@ -129,6 +129,19 @@ int celv2_set_output(celv2_engine* e, int job, celv2_sb_out* records);
 int celv2_host_alloc(long long bytes, void** out);
 int celv2_host_free(void* p);
 
+/* ---- Pruned search ----
+ * No counterpart in the reference. celv2_set_keep gives the NEXT launch's job (numbered as for
+ * celv2_set_output) one byte per superblock (sb_cols * sb_rows, raster order; NULL: exhaustive):
+ * bit r keeps reference r, bit 7 keeps the intra modes. A superblock then scores only what it
+ * keeps -- exactly as the exhaustive search scores it -- and picks among that: its pruned
+ * references' records read CELV2_NO_REF_COST, and with intra pruned no block is intra. An inter
+ * frame's superblock that keeps no reference keeps them all; a KEY frame always scores intra. The
+ * motion search skips the level-0 cells no superblock's kept references read.
+ * celv2_sb_costs copies the last launch's per-superblock cost of the chosen partition (the sum the
+ * partition choice minimises, lambda-weighted SATD plus rate) for one job; it waits for the work. */
+int celv2_set_keep(celv2_engine* e, int job, const uint8_t* keep);
+int celv2_sb_costs(celv2_engine* e, int job, int64_t* out);
+
 /* ---- A KEY-frame decision that allocates nothing ----
  * No counterpart in the reference. For callers that cannot allocate device memory while they run
  * (a host application that provisions all GPU memory up front, a path that cannot take the device

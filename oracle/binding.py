@@ -66,6 +66,9 @@ class Oracle:
         L.oro_decide.restype = C.c_int
         L.oro_decide.argtypes = [C.POINTER(C.c_uint8), C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_uint8)), C.c_int,
                                  C.c_int64, C.c_int, C.c_void_p]
+        L.oro_decide_masked.restype = C.c_int
+        L.oro_decide_masked.argtypes = [C.POINTER(C.c_uint8), C.c_int, C.c_int, C.POINTER(C.POINTER(C.c_uint8)),
+                                        C.c_int, C.c_int64, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.oro_build_pyramid.argtypes = [C.POINTER(C.c_uint8), C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint8)]
         L.oro_me_fields.argtypes = [C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), C.c_int, C.c_int,
                                     C.POINTER(C.POINTER(C.c_int32)), C.POINTER(C.POINTER(C.c_int32))]
@@ -91,6 +94,22 @@ class Oracle:
         if rc != 0:
             raise ValueError("oracle rejected the arguments")
         return out
+
+    def decide_masked(self, width: int, height: int, src_y: np.ndarray, refs_y, lam: int, keep=None,
+                      threads: int = 0):
+        """(records, per-superblock costs) with pruning masks (oro_decide_masked)."""
+        src_y = np.ascontiguousarray(src_y, dtype=np.uint8)
+        refs_y = [np.ascontiguousarray(r, dtype=np.uint8) for r in refs_y]
+        nsb = ((width + 63) // 64) * ((height + 63) // 64)
+        out = np.zeros(nsb, dtype=SB_OUT_DTYPE)
+        cost = np.zeros(nsb, dtype=np.int64)
+        k = None if keep is None else np.ascontiguousarray(keep, dtype=np.uint8)
+        rc = self.lib.oro_decide_masked(_u8p(src_y), width, height, _plist(refs_y), len(refs_y), int(lam), threads,
+                                        None if k is None else k.ctypes.data_as(C.c_void_p),
+                                        out.ctypes.data_as(C.c_void_p), cost.ctypes.data_as(C.c_void_p))
+        if rc != 0:
+            raise ValueError("oracle rejected the arguments")
+        return out, cost
 
     def pyramid(self, y: np.ndarray, phases: bool) -> np.ndarray:
         ph, pw = y.shape

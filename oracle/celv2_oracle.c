@@ -507,7 +507,7 @@ static best_t make_best(int64_t cost, int mode, int mvx, int mvy, int ref) {
  * all first strict minimum; records the block's candidates into o[b]; returns the block's best
  * (inter only where strictly cheaper than intra). */
 static best_t block_best(const plane_t* s, const refset_t* rs, int ox, int oy, int b, int64_t lam, int intra,
-                         celv2_sb_out* o) {
+                         unsigned keep_refs, celv2_sb_out* o) {
   int bx, by, w, h;
   oro_sb_block_geom(b, &bx, &by, &w, &h);
   const int x = ox + bx, y = oy + by;
@@ -521,6 +521,7 @@ static best_t block_best(const plane_t* s, const refset_t* rs, int ox, int oy, i
   const int ncand = mv_cells(x, y, w, h) + 8;
   for (int r = 0; r < rs->n; r++) {
     per[r] = make_best(INT64_MAX, kNumModes, 0, 0, r);
+    if (!(keep_refs >> r & 1u)) continue; /* a pruned reference is no candidate */
     for (int k = 0; k < ncand; k++) {
       if (repeated(rs->fx[r], rs->fy[r], rs->cols, rs->rows, x, y, w, h, k)) continue;
       const int i = candidate_index(x, y, w, h, k, rs->cols, rs->rows);
@@ -531,7 +532,7 @@ static best_t block_best(const plane_t* s, const refset_t* rs, int ox, int oy, i
     if (a < 0 || per[r].cost < per[a].cost) a = r;
   }
   for (int r = 0; r < rs->n; r++)
-    if (r != a && (second < 0 || per[r].cost < per[second].cost)) second = r;
+    if (r != a && (keep_refs >> r & 1u) && (second < 0 || per[r].cost < per[second].cost)) second = r;
   if (a >= 0) be = per[a];
   if (second >= 0 && compound_pair_ok(a, second, rs->n)) {
     const best_t p = per[a], q = per[second];
@@ -599,7 +600,8 @@ static void emit_square(celv2_sb_out* o, const int* choice, const best_t* best, 
 /* decide_sb_ref + decide_square (kernels_ref.cpp:125-198,253-270): every block's best, then per
  * square NONE / HORZ / VERT / SPLIT bottom-up (first strict minimum; the 64x64 square takes NONE,
  * HORZ or VERT only in inter frames, 8x8 squares never split), then the preorder tree. */
-static void decide_sb(const plane_t* s, const refset_t* rs, int sb_col, int sb_row, int64_t lam, celv2_sb_out* o) {
+static void decide_sb(const plane_t* s, const refset_t* rs, int sb_col, int sb_row, int64_t lam, unsigned keep,
+                      celv2_sb_out* o, int64_t* sb_cost) {
   blank_record(o);
   const int ox = sb_col * 64, oy = sb_row * 64;
   best_t best[kBlocks];
@@ -608,7 +610,7 @@ static void decide_sb(const plane_t* s, const refset_t* rs, int sb_col, int sb_r
       best[b] = make_best(INT64_MAX, 0, 0, 0, 0);
       continue;
     }
-    best[b] = block_best(s, rs, ox, oy, b, lam, b >= 5, o);
+    best[b] = block_best(s, rs, ox, oy, b, lam, b >= 5 && (keep & 0x80u), keep & 0x7fu, o);
   }
   int64_t sq_cost[CELV2_SB_SQUARES];
   int choice[CELV2_SB_SQUARES];
@@ -636,11 +638,23 @@ static void decide_sb(const plane_t* s, const refset_t* rs, int sb_col, int sb_r
       sq_cost[sq] = c, choice[sq] = ch;
     }
   }
+  if (sb_cost) *sb_cost = sq_cost[0];
   emit_square(o, choice, best, 0, 0, 0);
 }
 
+/* Pruning (an extension for testing the engine's pruned search, not a reference rule): the
+ * effective mask of a superblock -- all options without masks or in a KEY frame; else the given
+ * references (all if none is given) and intra if bit 7 is set. */
+static unsigned keep_of(const uint8_t* keep, int sb, int nrefs) {
+  const unsigned all = (1u << nrefs) - 1u;
+  if (!keep || nrefs == 0) return all | 0x80u;
+  const unsigned k = keep[sb];
+  return ((k & all) ? (k & all) : all) | (k & 0x80u);
+}
+
 static int decide_frame(const uint8_t* src_y, int width, int height, const plane_t* ref_planes, int32_t* const* fx,
-                        int32_t* const* fy, int nrefs, int64_t lam, int threads, celv2_sb_out* out) {
+                        int32_t* const* fy, int nrefs, int64_t lam, int threads, const uint8_t* keep,
+                        celv2_sb_out* out, int64_t* sb_cost) {
   const int pw = (width + 7) & ~7, ph = (height + 7) & ~7;
   const int sb_cols = (width + 63) / 64, sb_rows = (height + 63) / 64;
   const plane_t s = {src_y, pw, pw, ph, 0};
@@ -654,7 +668,8 @@ static int decide_frame(const uint8_t* src_y, int width, int height, const plane
   (void)threads;
 #endif
 #pragma omp parallel for schedule(dynamic, 1)
-  for (int i = 0; i < sb_cols * sb_rows; i++) decide_sb(&s, &rs, i % sb_cols, i / sb_cols, lam, &out[i]);
+  for (int i = 0; i < sb_cols * sb_rows; i++)
+    decide_sb(&s, &rs, i % sb_cols, i / sb_cols, lam, keep_of(keep, i, nrefs), &out[i], sb_cost ? &sb_cost[i] : NULL);
   return 0;
 }
 
@@ -671,14 +686,20 @@ int oro_decide_from_fields(const uint8_t* src_y, int width, int height, const ui
     planes[r].phase = (size_t)pw * ph;
     fx[r] = (int32_t*)mvx0[r], fy[r] = (int32_t*)mvy0[r];
   }
-  return decide_frame(src_y, width, height, planes, fx, fy, nrefs, lambda_q8, threads, out);
+  return decide_frame(src_y, width, height, planes, fx, fy, nrefs, lambda_q8, threads, NULL, out, NULL);
 }
 
 int oro_decide(const uint8_t* src_y, int width, int height, const uint8_t* const* ref_y, int nrefs, int64_t lambda_q8,
                int threads, celv2_sb_out* out) {
+  return oro_decide_masked(src_y, width, height, ref_y, nrefs, lambda_q8, threads, NULL, out, NULL);
+}
+
+int oro_decide_masked(const uint8_t* src_y, int width, int height, const uint8_t* const* ref_y, int nrefs,
+                      int64_t lambda_q8, int threads, const uint8_t* keep, celv2_sb_out* out, int64_t* sb_cost) {
   if (width <= 0 || height <= 0 || nrefs < 0 || nrefs > CELV2_MAX_REFS) return -1;
   const int pw = (width + 7) & ~7, ph = (height + 7) & ~7;
-  if (nrefs == 0) return decide_frame(src_y, width, height, NULL, NULL, NULL, 0, lambda_q8, threads, out);
+  if (nrefs == 0)
+    return decide_frame(src_y, width, height, NULL, NULL, NULL, 0, lambda_q8, threads, keep, out, sb_cost);
   if (pw < 16 || ph < 16) return -1; /* the 5-level pyramid needs a 1x1 top level */
 #ifdef _OPENMP
   if (threads > 0) omp_set_num_threads(threads);
@@ -716,7 +737,7 @@ int oro_decide(const uint8_t* src_y, int width, int height, const uint8_t* const
     planes[r].p = rp, planes[r].stride = pw, planes[r].w = pw, planes[r].h = ph, planes[r].phase = Lr.phase;
     fx0[r] = mvx[0], fy0[r] = mvy[0];
   }
-  const int rc = decide_frame(src_y, width, height, planes, fx0, fy0, nrefs, lambda_q8, threads, out);
+  const int rc = decide_frame(src_y, width, height, planes, fx0, fy0, nrefs, lambda_q8, threads, keep, out, sb_cost);
   free(cur), free(refs), free(fields);
   return rc;
 }

@@ -51,6 +51,14 @@ void oro_me_fields(const uint8_t* cur_pyr, const uint8_t* ref_pyr, int pw, int p
 int oro_decide(const uint8_t* src_y, int width, int height, const uint8_t* const* ref_y, int nrefs,
                int64_t lambda_q8, int threads, celv2_sb_out* out);
 
+/* oro_decide with pruning masks (an extension for testing the engine's pruned search; no
+ * reference rule): keep (NULL: none) holds one byte per superblock, bit r keeping reference r and
+ * bit 7 the intra modes; an inter frame's superblock that keeps no reference keeps them all, a KEY
+ * frame always scores intra. A superblock scores what it keeps exactly as oro_decide does and
+ * picks among it. sb_cost (NULL: not written) receives each superblock's chosen partition cost. */
+int oro_decide_masked(const uint8_t* src_y, int width, int height, const uint8_t* const* ref_y, int nrefs,
+                      int64_t lambda_q8, int threads, const uint8_t* keep, celv2_sb_out* out, int64_t* sb_cost);
+
 /* The same from prebuilt pyramids and level-0 fields (for the stage-by-stage tests). */
 int oro_decide_from_fields(const uint8_t* src_y, int width, int height, const uint8_t* const* ref_pyr,
                            const int32_t* const* mvx0, const int32_t* const* mvy0, int nrefs, int64_t lambda_q8,
