@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "celv2_cuda.h"
+#include "celv2_pruner.h"
 #include "kernels.h"
 #include "tables.h"
 
@@ -175,7 +176,19 @@ struct Stage {
 
 // Stages timed by CUDA events when stage timing is on (celv2_stage_timing).
 enum StageId { kStUpload, kStPhases, kStMe4, kStMe3, kStMe2, kStMe1, kStMe0, kStIntra, kStInter, kStFinalize, kStRefine,
-               kStages };
+               kStPruner, kStages };
+
+// A job's learned-pruner work, queued between motion-search levels 1 and 0: its features into
+// `feats` (when non-null), and with `net` the network's forward pass (cache `acts`) and the masks
+// into `keep`.
+struct NetJob {
+  float* feats = nullptr;
+  bool net = false;
+  const float* params = nullptr;
+  float* acts = nullptr;
+  uint8_t* keep = nullptr;
+  float tr = 0, ti = 0, band = 0;
+};
 
 // Per-frame device buffers of a decision.
 struct JobBuffers {
@@ -186,6 +199,7 @@ struct JobBuffers {
   celv2_sb_out* out2 = nullptr;  // group buffers: the records of every other group (see group_parity)
   uint8_t* keep = nullptr;       // pruning masks of the job, when given (nsb)
   long long* sb_cost = nullptr;  // per superblock, the chosen partition's cost (nsb)
+  float* feats = nullptr;        // the learned pruner's features (nsb x CELV2_PRUNER_FEATURES)
 };
 
 }  // namespace
@@ -254,6 +268,22 @@ struct celv2_engine {
   bool persistent = true;      // the queue-draining persistent stage kernels (else one CTA per unit)
   unsigned persistent_off = 0; // stages (bit i: queue i) that run one CTA per unit anyway
   int me_cells[kLevels] = {32, 32, 32, 32, 32};
+  // the learned pruner: features on request, the network when parameters are set
+  bool features_on = false;
+  float* pruner_params = nullptr;  // device, CELV2_PRUNER_PARAMS floats
+  float* nn_acts = nullptr;        // device, nsb x CELV2_PRUNER_ACTS floats
+  float pruner_tr = 0.5f, pruner_ti = 0.5f, pruner_band = 0.f;
+
+  // The pruner work of a job of this engine (buffers b; keep_given: celv2_set_keep masks win).
+  NetJob net_for(const FrameJob& job, const JobBuffers& b, bool keep_given) const {
+    NetJob n;
+    if (job.nrefs == 0) return n;
+    const bool net = pruner_params && !keep_given;
+    if (!features_on && !net) return n;
+    n.feats = b.feats, n.net = net, n.params = pruner_params, n.acts = nn_acts, n.keep = b.keep;
+    n.tr = pruner_tr, n.ti = pruner_ti, n.band = pruner_band;
+    return n;
+  }
   int inter_chunk = 64;
 
   template <typename F>
@@ -311,6 +341,8 @@ struct celv2_engine {
     for (const Timed& t : timed) cudaEventDestroy(t.a), cudaEventDestroy(t.b);
     cudaFree(stats);
     cudaFree(queues);
+    cudaFree(pruner_params);
+    cudaFree(nn_acts);
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     cudaFree(djobs);
     cudaFreeHost(ring);
@@ -335,7 +367,7 @@ struct celv2_engine {
 
   static void free_buffers(JobBuffers& b) {
     cudaFree(b.fields), cudaFree(b.intra), cudaFree(b.inter), cudaFree(b.out), cudaFree(b.out2);
-    cudaFree(b.keep), cudaFree(b.sb_cost);
+    cudaFree(b.keep), cudaFree(b.sb_cost), cudaFree(b.feats);
     b = JobBuffers{};
   }
 
@@ -347,6 +379,7 @@ struct celv2_engine {
     if (with_intra) CK(cudaMalloc(&b.out2, (size_t)g.nsb * sizeof(celv2_sb_out)));
     CK(cudaMalloc(&b.keep, (size_t)g.nsb));
     CK(cudaMalloc(&b.sb_cost, (size_t)g.nsb * sizeof(long long)));
+    CK(cudaMalloc(&b.feats, (size_t)g.nsb * CELV2_PRUNER_FEATURES * sizeof(float)));
   }
 
   void init(int width, int height, int dev) {
@@ -538,7 +571,8 @@ struct celv2_engine {
 
   // Queues the stage kernels of the jobs whose descriptors are in djobs (intra for all of them
   // or none); returns the kernels launched.
-  int enqueue_stages(const std::vector<FrameJob>& jobs, bool with_intra, cudaStream_t stream) {
+  int enqueue_stages(const std::vector<FrameJob>& jobs, bool with_intra, cudaStream_t stream,
+                     const std::vector<NetJob>& nets) {
     const int n = (int)jobs.size();
     int launched = 0;
     if (persistent) CK(cudaMemsetAsync(queues, 0, 9 * sizeof(unsigned), stream));
@@ -548,6 +582,21 @@ struct celv2_engine {
     for (int l = kLevels - 1; l >= 0; l--) {
       for (int j = 0; j < n; j++)
         w.prefix[j + 1] = w.prefix[j] + me_units(jobs[j].nrefs, jobs[j].fcols[l], jobs[j].frows[l], me_cells[l]);
+      if (l == 0)  // the learned pruner's masks, from the level-1 motion search, before level 0
+        for (int j = 0; j < n && j < (int)nets.size(); j++) {
+          const NetJob& nj = nets[j];
+          if (!nj.feats) continue;
+          const int nsb = jobs[j].sb_cols * jobs[j].sb_rows;
+          stage(kStPruner, stream, [&] {
+            launch_features(djobs + j, nsb, nj.feats, stream);
+            if (nj.net) {
+              pruner_forward(nj.params, nj.feats, nsb, nj.acts, stream);
+              launch_masks(nj.acts + (size_t)nsb * (CELV2_PRUNER_ACTS - CELV2_PRUNER_OUTPUTS), nsb, jobs[j].nrefs,
+                           nj.tr, nj.ti, nj.band, nj.keep, stream);
+            }
+          });
+          launched += nj.net ? 16 : 1;
+        }
       w.queue = q(l);
       if (w.prefix[n] > 0) {
         stage(kStMe0 - l, stream, [&] { launch_me_level(djobs, w, l, me_cells[l], stream); });
@@ -582,9 +631,10 @@ struct celv2_engine {
   }
 
   // The stage kernels of the jobs, their descriptors sent through the pinned ring.
-  void run_stages(const std::vector<FrameJob>& jobs, bool with_intra, cudaStream_t stream) {
+  void run_stages(const std::vector<FrameJob>& jobs, bool with_intra, cudaStream_t stream,
+                  const std::vector<NetJob>& nets = {}) {
     put_jobs(jobs.data(), (int)jobs.size(), djobs, stream);
-    kernel_launches += enqueue_stages(jobs, with_intra, stream);
+    kernel_launches += enqueue_stages(jobs, with_intra, stream, nets);
   }
 
   void wait_idle() {
@@ -642,7 +692,9 @@ struct celv2_engine {
       std::vector<FrameJob> jobs(1);
       fill_job(jobs[0], srcs[use].pyr, used, nrefs, single, intra_prep[use], lam);
       jobs[0].keep = put_keep(keep0, single, st);
-      run_stages(jobs, !prepared, st);
+      const std::vector<NetJob> nets{net_for(jobs[0], single, !keep0.empty())};
+      if (nets[0].net) jobs[0].keep = single.keep;
+      run_stages(jobs, !prepared, st, nets);
       mark_used(used, nrefs, st);
       last_nrefs = nrefs;
       // rows back to the host in row-stream order
@@ -812,13 +864,18 @@ struct celv2_engine {
       }
       fill_job(jobs[j], cur->pyr, refs, nrefs[j], group[j], group[j].intra, lams[j]);
     }
-    for (int j = 0; j < njobs; j++) jobs[j].keep = put_keep(keeps[j], group[j], st);
+    std::vector<NetJob> nets(njobs);
+    for (int j = 0; j < njobs; j++) {
+      jobs[j].keep = put_keep(keeps[j], group[j], st);
+      nets[j] = net_for(jobs[j], group[j], !keeps[j].empty());
+      if (nets[j].net) jobs[j].keep = group[j].keep;
+    }
     const int par = take_parity(st);
     for (int j = 0; j < njobs; j++) jobs[j].out = par ? group[j].out2 : group[j].out;
     if (use_graphs && !timing)
-      launch_graph(jobs);
+      launch_graph(jobs, nets);
     else
-      run_stages(jobs, true, st);
+      run_stages(jobs, true, st, nets);
     mark_used(reads.data(), (int)reads.size(), st);
     if (to_host) {
       CK(cudaEventRecord(stages_done, st));
@@ -859,9 +916,10 @@ struct celv2_engine {
     graphs.clear();
   }
 
-  void launch_graph(const std::vector<FrameJob>& jobs) {
+  void launch_graph(const std::vector<FrameJob>& jobs, const std::vector<NetJob>& nets) {
     std::vector<int> key;
-    for (const FrameJob& j : jobs) key.push_back(j.nrefs);
+    for (size_t j = 0; j < jobs.size(); j++)
+      key.push_back(jobs[j].nrefs * 4 + (nets[j].feats ? 2 : 0) + (nets[j].net ? 1 : 0));
     Graph* gr = nullptr;
     for (Graph& x : graphs)
       if (x.key == key) gr = &x;
@@ -876,7 +934,7 @@ struct celv2_engine {
       CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       try {
         CK(cudaMemcpyAsync(djobs, gr->host_jobs, n * sizeof(FrameJob), cudaMemcpyHostToDevice, st));
-        gr->kernels = enqueue_stages(jobs, true, st);
+        gr->kernels = enqueue_stages(jobs, true, st, nets);
       } catch (...) {
         cudaStreamEndCapture(st, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -932,6 +990,7 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     }
   struct Entry {
     FrameJob job;
+    NetJob net;
     celv2_engine* e;
     int slot;
     long long work;
@@ -965,6 +1024,8 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     Entry en;
     e->fill_job(en.job, cur->pyr, refs, nrefs[j], e->group[slot], e->group[slot].intra, lams[j]);
     en.job.keep = e->put_keep(keeps[ei][slot], e->group[slot], lead->st);
+    en.net = e->net_for(en.job, e->group[slot], !keeps[ei][slot].empty());
+    if (en.net.net) en.job.keep = e->group[slot].keep;
     en.job.out = par[ei] ? e->group[slot].out2 : e->group[slot].out;
     en.e = e, en.slot = slot, en.work = (long long)(nrefs[j] + 1) * e->g.nsb, en.dest = dests[ei][slot];
     entries.push_back(en);
@@ -972,8 +1033,9 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
   // the largest jobs first, so the queues' last units are small ones
   std::stable_sort(entries.begin(), entries.end(), [](const Entry& a, const Entry& b) { return a.work > b.work; });
   std::vector<FrameJob> jobs;
-  for (const Entry& en : entries) jobs.push_back(en.job);
-  lead->run_stages(jobs, true, lead->st);
+  std::vector<NetJob> nets;
+  for (const Entry& en : entries) jobs.push_back(en.job), nets.push_back(en.net);
+  lead->run_stages(jobs, true, lead->st, nets);
   for (size_t i = 0; i < uniq.size(); i++) uniq[i]->mark_used(reads[i].data(), (int)reads[i].size(), lead->st);
   if (to_host) {  // on the lead's copy stream, overlapping later work
     CK(cudaEventRecord(lead->stages_done, lead->st));
@@ -1250,6 +1312,58 @@ int celv2_debug_inter(celv2_engine* e, int32_t* out) {
 
 long long celv2_kernel_launches(const celv2_engine* e) { return e ? e->kernel_launches : 0; }
 
+int celv2_set_pruner(celv2_engine* e, const float* params, float ref_threshold, float intra_threshold, float band) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    if (params && !(ref_threshold >= 0.f && ref_threshold <= 1.f && intra_threshold >= 0.f && intra_threshold <= 1.f &&
+                    band >= 0.f))
+      invalid("set_pruner: thresholds must lie in [0, 1] and the band be >= 0");
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    e->free_graphs();  // captured batches hold the old settings
+    if (!params) {
+      cudaFree(e->pruner_params), cudaFree(e->nn_acts);
+      e->pruner_params = nullptr, e->nn_acts = nullptr;
+      return;
+    }
+    if (!e->pruner_params) {
+      CK(cudaMalloc(&e->pruner_params, CELV2_PRUNER_PARAMS * sizeof(float)));
+      CK(cudaMalloc(&e->nn_acts, (size_t)e->g.nsb * CELV2_PRUNER_ACTS * sizeof(float)));
+    }
+    CK(cudaMemcpy(e->pruner_params, params, CELV2_PRUNER_PARAMS * sizeof(float), cudaMemcpyHostToDevice));
+    e->pruner_tr = ref_threshold, e->pruner_ti = intra_threshold, e->pruner_band = band;
+  });
+}
+
+namespace {
+// The buffers of job `job` of the last launch (a group's, or launch()'s own).
+const JobBuffers& last_buffers(const celv2_engine* e, int job) {
+  const bool group = e->group_jobs > 0 && e->launches_group == e->launches;
+  if (job < 0 || (group ? job >= e->group_jobs : job != 0)) invalid("no such job in the last launch");
+  return group ? e->group[job] : e->single;
+}
+}  // namespace
+
+int celv2_features(celv2_engine* e, int job, float* out) {
+  return guarded([&] {
+    if (!e || !out) invalid("null argument");
+    const JobBuffers& b = last_buffers(e, job);
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    CK(cudaMemcpy(out, b.feats, (size_t)e->g.nsb * CELV2_PRUNER_FEATURES * sizeof(float), cudaMemcpyDeviceToHost));
+  });
+}
+
+int celv2_pruner_masks(celv2_engine* e, int job, uint8_t* out) {
+  return guarded([&] {
+    if (!e || !out) invalid("null argument");
+    const JobBuffers& b = last_buffers(e, job);
+    CK(cudaSetDevice(e->device));
+    e->wait_idle();
+    CK(cudaMemcpy(out, b.keep, (size_t)e->g.nsb, cudaMemcpyDeviceToHost));
+  });
+}
+
 int celv2_set_config(celv2_engine* e, int key, int value) {
   return guarded([&] {
     if (!e) invalid("null engine");
@@ -1258,6 +1372,7 @@ int celv2_set_config(celv2_engine* e, int key, int value) {
     switch (key) {
       case CELV2_CFG_PERSISTENT: e->persistent = value != 0, e->free_graphs(); break;
       case CELV2_CFG_GRAPHS: e->use_graphs = value != 0; break;
+      case CELV2_CFG_FEATURES: e->features_on = value != 0, e->free_graphs(); break;
       case CELV2_CFG_PERSISTENT_OFF: e->persistent_off = (unsigned)value & 0x1ff, e->free_graphs(); break;
       case CELV2_CFG_INTER_CHUNK:
         if (value < 8 || value > 64) invalid("inter chunk must be 8..64");
@@ -1281,6 +1396,7 @@ int celv2_get_config(const celv2_engine* e, int key, int* value) {
     if (!e || !value) invalid("null argument");
     switch (key) {
       case CELV2_CFG_PERSISTENT: *value = e->persistent; break;
+      case CELV2_CFG_FEATURES: *value = e->features_on; break;
       case CELV2_CFG_GRAPHS: *value = e->use_graphs; break;
       case CELV2_CFG_PERSISTENT_OFF: *value = (int)e->persistent_off; break;
       case CELV2_CFG_INTER_CHUNK: *value = e->inter_chunk; break;

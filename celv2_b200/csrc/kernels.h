@@ -72,6 +72,13 @@ void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, cudaStream
 // Per-block choice, compound, partition choice and the decision records. Units: superblocks.
 void launch_finalize(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
 
+// The learned pruner (pruner.cu): one job's features (nsb x CELV2_PRUNER_FEATURES), the network's
+// forward pass into a cache of batch x CELV2_PRUNER_ACTS floats (logits last), and the masks.
+void launch_features(const FrameJob* djob, int nsb, float* out, cudaStream_t st);
+void pruner_forward(const float* params, const float* x, int batch, float* acts, cudaStream_t st);
+void launch_masks(const float* logits, int nsb, int nrefs, float tr, float ti, float band, uint8_t* keep,
+                  cudaStream_t st);
+
 // Set-up of the constant tables (once per device).
 cudaError_t init_tables();
 

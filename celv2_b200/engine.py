@@ -76,13 +76,26 @@ SIGNATURES = {
     "celv2_host_alloc": (C.c_int, [C.c_longlong, C.POINTER(C.c_void_p)]),
     "celv2_host_free": (C.c_int, [C.c_void_p]),
     "celv2_set_keep": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    # include/celv2_pruner.h
+    "celv2_pruner_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "celv2_pruner_backward": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    "celv2_pruner_bce": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]),
+    "celv2_pruner_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
+                                    C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]),
+    "celv2_set_pruner": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float]),
+    "celv2_features": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "celv2_pruner_masks": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "celv2_sb_costs": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
 }
 
-CFG_PERSISTENT, CFG_GRAPHS, CFG_PERSISTENT_OFF, CFG_INTER_CHUNK, CFG_ME_CELLS_L0 = 1, 2, 3, 4, 10
+CFG_PERSISTENT, CFG_GRAPHS, CFG_PERSISTENT_OFF, CFG_INTER_CHUNK, CFG_FEATURES, CFG_ME_CELLS_L0 = 1, 2, 3, 4, 5, 10
+
+PRUNER_FEATURES, PRUNER_OUTPUTS, PRUNER_PARAMS, PRUNER_ACTS, PRUNER_WORK = 376, 8, 55080, 23488, 20544
 
 STAGE_NAMES = ["upload+pyramid", "phases", "me_l4", "me_l3", "me_l2", "me_l1", "me_l0", "intra", "inter",
-               "finalize", "me_refine"]
+               "finalize", "me_refine", "pruner"]
 
 
 def library():
@@ -385,6 +398,30 @@ class CudaEngine:
         if k.size != self.sb_cols * self.sb_rows:
             raise ValueError("set_keep: one byte per superblock")
         _check(library().celv2_set_keep(self._h, job, k.ctypes.data))
+
+    def set_pruner(self, params, ref_threshold: float = 0.5, intra_threshold: float = 0.5,
+                   band: float = 0.0) -> None:
+        """celv2_set_pruner: the learned pruner (FP32 parameters, CELV2_PRUNER_PARAMS) scores every
+        later inter frame on its own masks; None turns it off."""
+        if params is None:
+            _check(library().celv2_set_pruner(self._h, None, 0.0, 0.0, 0.0))
+            return
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        if p.size != PRUNER_PARAMS:
+            raise ValueError(f"set_pruner: {PRUNER_PARAMS} parameters")
+        _check(library().celv2_set_pruner(self._h, p.ctypes.data, ref_threshold, intra_threshold, band))
+
+    def features(self, job: int = 0) -> np.ndarray:
+        """The last launch's learned-pruner features of job (nsb x CELV2_PRUNER_FEATURES)."""
+        out = np.empty((self.sb_cols * self.sb_rows, PRUNER_FEATURES), dtype=np.float32)
+        _check(library().celv2_features(self._h, job, out.ctypes.data))
+        return out
+
+    def pruner_masks(self, job: int = 0) -> np.ndarray:
+        """The masks the pruner chose for the last launch's job (one byte per superblock)."""
+        out = np.empty(self.sb_cols * self.sb_rows, dtype=np.uint8)
+        _check(library().celv2_pruner_masks(self._h, job, out.ctypes.data))
+        return out
 
     def sb_costs(self, job: int = 0) -> np.ndarray:
         """The last launch's per-superblock cost of the chosen partition (int64), job's."""

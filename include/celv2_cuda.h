@@ -182,12 +182,15 @@ long long celv2_kernel_launches(const celv2_engine* e);
  *  CELV2_CFG_INTER_CHUNK: distinct MVs per pass of the inter stage, 8..64 (default 64).
  *  CELV2_CFG_ME_CELLS_L0 + l: 8x8 cells per motion-search CTA at pyramid level l, 16 or 32
  *    (default 32).
+ *  CELV2_CFG_FEATURES: 1 -- every inter frame's learned-pruner features are kept for
+ *    celv2_features (include/celv2_pruner.h); 0 (default) -- only when the pruner runs.
  * The autotuner (celv2_b200/tune.py) times these per frame size and sets the fastest. */
 enum {
   CELV2_CFG_PERSISTENT = 1,
   CELV2_CFG_GRAPHS = 2,
   CELV2_CFG_PERSISTENT_OFF = 3,
   CELV2_CFG_INTER_CHUNK = 4,
+  CELV2_CFG_FEATURES = 5,
   CELV2_CFG_ME_CELLS_L0 = 10,
 };
 int celv2_set_config(celv2_engine* e, int key, int value);
@@ -200,8 +203,9 @@ int celv2_stream(const celv2_engine* e, void** stream);
 /* Stage timing: when enabled, every stage launch is bracketed by CUDA events on its stream.
  * celv2_stage_times returns (and resets) the summed milliseconds and launch counts per stage, in
  * the order: uploads (8-bit level 0 + pyramid), quarter-pel phases, motion search levels 4, 3, 2,
- * 1, 0, intra, inter, finalize, level 0's quarter-pel refinement (CELV2_STAGES entries). */
-#define CELV2_STAGES 11
+ * 1, 0, intra, inter, finalize, level 0's quarter-pel refinement, the learned pruner (CELV2_STAGES
+ * entries). */
+#define CELV2_STAGES 12
 int celv2_stage_timing(celv2_engine* e, int enable);
 int celv2_stage_times(celv2_engine* e, double* ms, long long* launches, int n);
 /* Work the kernels executed while stage timing was on, then reset: [l] motion-search centres

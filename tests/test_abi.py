@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = []
-    for h in ("celv2_cuda.h",):
+    for h in ("celv2_cuda.h", "celv2_pruner.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names += re.findall(r"\b(celv2_[a-z_0-9]+)\s*\(", text)

@@ -1,0 +1,165 @@
+"""The learned pruner's CUDA kernels against their CPU restatement (oracle/pruner_ref.py): the
+tensor-core forward pass, every parameter's gradient, the loss, the Adam step and the features;
+then the engine running the network: its masks are the network's, applied exactly."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import frames as F
+from celv2_b200 import engine as E
+from celv2_b200 import lam
+from celv2_b200.pruner import net as N
+from celv2_b200.records import first_difference, records_equal
+from oracle import pruner_ref as R
+from oracle.binding import field_dims
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
+
+
+def ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def case(batch, seed=0):
+    rng = np.random.default_rng(seed)
+    p = N.init_params(seed) + rng.normal(0, 0.02, E.PRUNER_PARAMS).astype(np.float32)  # biases not all zero
+    x = rng.normal(0, 1, (batch, E.PRUNER_FEATURES)).astype(np.float32)
+    return p, x
+
+
+@pytest.mark.parametrize("batch", [1, 37, 300])
+def test_forward_matches_oracle(batch):
+    p, x = case(batch)
+    tr = N.Trainer(batch, params=p)
+    got = tr.logits(dev(x)).cpu().numpy()
+    want, _ = R.forward(p, x, bf=True)
+    assert np.allclose(got, want, rtol=1e-3, atol=1e-3), np.abs(got - want).max()
+
+
+@pytest.mark.parametrize("batch", [5, 64, 129])
+def test_backward_matches_oracle(batch):
+    p, x = case(batch, seed=batch)
+    rng = np.random.default_rng(batch + 1)
+    dl = rng.normal(0, 1, (batch, 8)).astype(np.float32)
+    tr = N.Trainer(batch, params=p)
+    xt = dev(x)
+    tr.logits(xt)
+    lib = E.library()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    assert lib.celv2_pruner_backward(ptr(tr.p), batch, ptr(tr.acts), ptr(dev(dl)), ptr(tr.work), ptr(tr.g), st) == 0
+    got = tr.g.cpu().numpy()
+    _, cache = R.forward(p, x, bf=True)
+    want = R.backward(p, cache, dl, bf=True)
+    o = 0
+    for name, shape in R.SHAPES:
+        n = int(np.prod(shape))
+        g, w = got[o:o + n], want[o:o + n]
+        err = np.linalg.norm(g - w) / max(np.linalg.norm(w), 1e-12)
+        assert err < 2e-3, (name, err)
+        o += n
+
+
+def test_loss_and_adam_match_oracle():
+    rng = np.random.default_rng(7)
+    z = rng.normal(0, 2, (50, 8)).astype(np.float32)
+    y = (rng.random((50, 8)) < 0.4).astype(np.float32)
+    w = rng.choice([0.0, 1.0, 2.0], (50, 8)).astype(np.float32)
+    lib = E.library()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    dz, loss = torch.zeros(400, device="cuda"), torch.zeros(1, device="cuda")
+    assert lib.celv2_pruner_bce(ptr(dev(z)), ptr(dev(y)), ptr(dev(w)), 50, ptr(dz), ptr(loss), st) == 0
+    want_loss, want_dz = R.bce(z, y, w)
+    assert abs(loss.item() - want_loss) < 1e-4 * max(1.0, abs(want_loss))
+    assert np.allclose(dz.cpu().numpy().reshape(50, 8), want_dz, atol=1e-6)
+    p = rng.normal(0, 1, 1000).astype(np.float32)
+    g = rng.normal(0, 1, 1000).astype(np.float32)
+    pt, gt, m, v = dev(p), dev(g), torch.zeros(1000, device="cuda"), torch.zeros(1000, device="cuda")
+    for step in (1, 2):
+        assert lib.celv2_pruner_adam(ptr(pt), ptr(gt), ptr(m), ptr(v), 1000, 1e-2, 0.9, 0.999, 1e-8, 1e-4, step,
+                                     st) == 0
+    mm, vv, q = np.zeros(1000), np.zeros(1000), p.astype(np.float64)
+    for step in (1, 2):
+        mm = 0.9 * mm + 0.1 * g
+        vv = 0.999 * vv + 0.001 * g * g
+        q -= 1e-2 * ((mm / (1 - 0.9 ** step)) / (np.sqrt(vv / (1 - 0.999 ** step)) + 1e-8) + 1e-4 * q)
+    assert np.allclose(pt.cpu().numpy(), q, atol=1e-5)
+
+
+def levels(pyr, pw, ph):
+    out, o, w, h = [], 0, pw, ph
+    for _ in range(5):
+        out.append(pyr[o:o + w * h].reshape(h, w))
+        o += w * h
+        w, h = w // 2, h // 2
+    return out
+
+
+def test_features_match_oracle(oracle):
+    w, h = 202, 122
+    src = F.textured(w, h, 5, -3)
+    refs = [F.textured(w, h, i, -(i // 2)) for i in range(3)]
+    pw, ph = (w + 7) & ~7, (h + 7) & ~7
+    with E.CudaEngine(w, h) as e:
+        e.set_config(E.CFG_FEATURES, 1)
+        e.decide_inter(src, refs, 120)
+        got = e.features(0)
+    cur = levels(oracle.pyramid(src, False), pw, ph)
+    cols, rows = field_dims(pw, ph)
+    sbc, sbr = (w + 63) // 64, (h + 63) // 64
+    want = np.zeros((sbc * sbr, E.PRUNER_FEATURES), np.float32)
+
+    def clamp_read(pl, y, x):
+        return pl[np.clip(y, 0, pl.shape[0] - 1), np.clip(x, 0, pl.shape[1] - 1)].astype(np.int64)
+
+    fields = [oracle.me_fields(src, r) for r in refs]
+    ref1 = [levels(oracle.pyramid(r, False), pw, ph)[1] for r in refs]
+    for sb in range(sbc * sbr):
+        sy, sx = divmod(sb, sbc)
+        yy, xx = np.mgrid[0:16, 0:16]
+        v = clamp_read(cur[2], sy * 16 + yy, sx * 16 + xx).astype(np.float32)
+        want[sb, :256] = ((v - np.float32(v.sum() / 256.0)) / np.float32(64)).reshape(-1)
+        for r in range(3):
+            fx, fy = fields[r][1]
+            for cell in range(16):
+                cx, cy = min(sx * 4 + cell % 4, cols[1] - 1), min(sy * 4 + cell // 4, rows[1] - 1)
+                mx, my = int(fx[cy, cx]), int(fy[cy, cx])
+                iy, ix = np.mgrid[0:8, 0:8]
+                a = clamp_read(cur[1], cy * 8 + iy, cx * 8 + ix)
+                b = clamp_read(ref1[r], cy * 8 + my + iy, cx * 8 + mx + ix)
+                want[sb, 256 + r * 16 + cell] = np.log2(1.0 + np.abs(a - b).sum()) / 14.0
+        want[sb, 368:371] = 1.0
+        want[sb, 375] = np.log2(float(lam.lambda_q8(120))) / 20.0
+    assert np.allclose(got, want, atol=2e-6), np.abs(got - want).max()
+
+
+def test_engine_applies_the_networks_masks(oracle):
+    """With the pruner on, the records are the oracle's for the masks the network chose, and the
+    masks are what the network's outputs and thresholds give."""
+    w, h = 640, 360
+    src = F.textured(w, h, 5, -3)
+    refs = [F.textured(w, h, i, -(i // 2)) for i in range(4)]
+    p, _ = case(1, seed=3)
+    with E.CudaEngine(w, h) as e:
+        e.set_config(E.CFG_FEATURES, 1)
+        e.decide_inter(src, refs, 120)
+        x = e.features(0)
+        e.set_pruner(p, 0.4, 0.5, 0.0)
+        got = e.decide_inter(src, refs, 120)
+        masks = e.pruner_masks(0)
+        costs = e.sb_costs(0)
+    z, _ = R.forward(p, x, bf=True)
+    prob = 1 / (1 + np.exp(-z.astype(np.float64)))
+    for sb in range(x.shape[0]):
+        pr = prob[sb, :4]
+        want = sum(1 << r for r in range(4) if pr[r] >= 0.4) | (1 << int(np.argmax(pr))) | (0x80 if prob[sb, 7] >= 0.5 else 0)
+        near = np.abs(pr - 0.4).min() < 1e-3 or abs(prob[sb, 7] - 0.5) < 1e-3  # rounding-order ties
+        assert near or masks[sb] == want, (sb, masks[sb], want)
+    want_rec, want_cost = oracle.decide_masked(w, h, src, refs, lam.lambda_q8(120), masks)
+    assert records_equal(got.records, want_rec), first_difference(got.records, want_rec)
+    assert (costs == want_cost).all()
