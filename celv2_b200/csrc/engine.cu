@@ -186,6 +186,7 @@ struct NetJob {
   bool net = false;
   const float* params = nullptr;
   float* acts = nullptr;
+  long long cap = 0;  // samples `acts` holds
   uint8_t* keep = nullptr;
   float tr = 0, ti = 0, band = 0;
 };
@@ -200,6 +201,7 @@ struct JobBuffers {
   uint8_t* keep = nullptr;       // pruning masks of the job, when given (nsb)
   long long* sb_cost = nullptr;  // per superblock, the chosen partition's cost (nsb)
   float* feats = nullptr;        // the learned pruner's features (nsb x CELV2_PRUNER_FEATURES)
+  bool owns_feats = false;       // group slots share one block (consecutive slots, consecutive rows)
 };
 
 }  // namespace
@@ -241,6 +243,7 @@ struct celv2_engine {
   // group path
   int group_cap = 0;
   std::vector<JobBuffers> group;
+  float* group_feats = nullptr;  // the group slots' pruner features, slot after slot
   celv2_sb_out* group_host = nullptr;
   int group_jobs = 0;
   // Group records go to the host on copy_st, overlapping the next group's stages, which write the
@@ -271,7 +274,8 @@ struct celv2_engine {
   // the learned pruner: features on request, the network when parameters are set
   bool features_on = false;
   float* pruner_params = nullptr;  // device, CELV2_PRUNER_PARAMS floats
-  float* nn_acts = nullptr;        // device, nsb x CELV2_PRUNER_ACTS floats
+  float* nn_acts = nullptr;        // device, nn_cap x CELV2_PRUNER_ACTS floats
+  long long nn_cap = 0;
   float pruner_tr = 0.5f, pruner_ti = 0.5f, pruner_band = 0.f;
 
   // The pruner work of a job of this engine (buffers b; keep_given: celv2_set_keep masks win).
@@ -280,7 +284,7 @@ struct celv2_engine {
     if (job.nrefs == 0) return n;
     const bool net = pruner_params && !keep_given;
     if (!features_on && !net) return n;
-    n.feats = b.feats, n.net = net, n.params = pruner_params, n.acts = nn_acts, n.keep = b.keep;
+    n.feats = b.feats, n.net = net, n.params = pruner_params, n.acts = nn_acts, n.cap = nn_cap, n.keep = b.keep;
     n.tr = pruner_tr, n.ti = pruner_ti, n.band = pruner_band;
     return n;
   }
@@ -343,6 +347,7 @@ struct celv2_engine {
     cudaFree(queues);
     cudaFree(pruner_params);
     cudaFree(nn_acts);
+    cudaFree(group_feats);
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     cudaFree(djobs);
     cudaFreeHost(ring);
@@ -367,7 +372,8 @@ struct celv2_engine {
 
   static void free_buffers(JobBuffers& b) {
     cudaFree(b.fields), cudaFree(b.intra), cudaFree(b.inter), cudaFree(b.out), cudaFree(b.out2);
-    cudaFree(b.keep), cudaFree(b.sb_cost), cudaFree(b.feats);
+    cudaFree(b.keep), cudaFree(b.sb_cost);
+    if (b.owns_feats) cudaFree(b.feats);
     b = JobBuffers{};
   }
 
@@ -379,7 +385,10 @@ struct celv2_engine {
     if (with_intra) CK(cudaMalloc(&b.out2, (size_t)g.nsb * sizeof(celv2_sb_out)));
     CK(cudaMalloc(&b.keep, (size_t)g.nsb));
     CK(cudaMalloc(&b.sb_cost, (size_t)g.nsb * sizeof(long long)));
-    CK(cudaMalloc(&b.feats, (size_t)g.nsb * CELV2_PRUNER_FEATURES * sizeof(float)));
+    if (!with_intra) {  // the group slots' features are one block (reserve_group)
+      CK(cudaMalloc(&b.feats, (size_t)g.nsb * CELV2_PRUNER_FEATURES * sizeof(float)));
+      b.owns_feats = true;
+    }
   }
 
   void init(int width, int height, int dev) {
@@ -582,21 +591,8 @@ struct celv2_engine {
     for (int l = kLevels - 1; l >= 0; l--) {
       for (int j = 0; j < n; j++)
         w.prefix[j + 1] = w.prefix[j] + me_units(jobs[j].nrefs, jobs[j].fcols[l], jobs[j].frows[l], me_cells[l]);
-      if (l == 0)  // the learned pruner's masks, from the level-1 motion search, before level 0
-        for (int j = 0; j < n && j < (int)nets.size(); j++) {
-          const NetJob& nj = nets[j];
-          if (!nj.feats) continue;
-          const int nsb = jobs[j].sb_cols * jobs[j].sb_rows;
-          stage(kStPruner, stream, [&] {
-            launch_features(djobs + j, nsb, nj.feats, stream);
-            if (nj.net) {
-              pruner_forward(nj.params, nj.feats, nsb, nj.acts, stream);
-              launch_masks(nj.acts + (size_t)nsb * (CELV2_PRUNER_ACTS - CELV2_PRUNER_OUTPUTS), nsb, jobs[j].nrefs,
-                           nj.tr, nj.ti, nj.band, nj.keep, stream);
-            }
-          });
-          launched += nj.net ? 16 : 1;
-        }
+      if (l == 0 && !nets.empty())  // the learned pruner, from the level-1 motion search
+        stage(kStPruner, stream, [&] { launched += enqueue_pruner(jobs, nets, stream); });
       w.queue = q(l);
       if (w.prefix[n] > 0) {
         stage(kStMe0 - l, stream, [&] { launch_me_level(djobs, w, l, me_cells[l], stream); });
@@ -627,6 +623,48 @@ struct celv2_engine {
     stage(kStFinalize, stream, [&] { launch_finalize(djobs, w, stream); });
     launched++;
     CK(cudaGetLastError());
+    return launched;
+  }
+
+  // The pruner's features per job, then its network over runs of consecutive jobs whose features
+  // are consecutive rows (a group's slots) and that share parameters, in chunks of the cache's
+  // capacity, then each job's masks; returns the kernels launched.
+  int enqueue_pruner(const std::vector<FrameJob>& jobs, const std::vector<NetJob>& nets, cudaStream_t stream) {
+    const int n = std::min((int)jobs.size(), (int)nets.size());
+    const long long F = CELV2_PRUNER_FEATURES;
+    int launched = 0;
+    auto nsb_of = [&](int j) { return (long long)jobs[j].sb_cols * jobs[j].sb_rows; };
+    for (int j = 0; j < n; j++)
+      if (nets[j].feats) launch_features(djobs + j, (int)nsb_of(j), nets[j].feats, stream), launched++;
+    for (int j = 0; j < n;) {
+      if (!nets[j].net) {
+        j++;
+        continue;
+      }
+      const NetJob& a = nets[j];
+      int k = j;
+      long long rows = nsb_of(j);
+      while (k + 1 < n && nets[k + 1].net && nets[k + 1].params == a.params && nets[k + 1].acts == a.acts &&
+             nets[k + 1].feats == nets[k].feats + nsb_of(k) * F)
+        rows += nsb_of(++k);
+      for (long long r0 = 0; r0 < rows; r0 += a.cap) {
+        const int cb = (int)std::min(a.cap, rows - r0);
+        pruner_forward(a.params, a.feats + r0 * F, cb, a.acts, stream);
+        launched += 12;
+        const float* logits = a.acts + (long long)cb * (CELV2_PRUNER_ACTS - CELV2_PRUNER_OUTPUTS);
+        long long base = 0;
+        for (int q = j; q <= k; q++) {
+          const long long lo = std::max(base, r0), hi = std::min(base + nsb_of(q), r0 + cb);
+          if (lo < hi) {
+            launch_masks(logits + (lo - r0) * CELV2_PRUNER_OUTPUTS, (int)(hi - lo), jobs[q].nrefs, nets[q].tr,
+                         nets[q].ti, nets[q].band, nets[q].keep + (lo - base), stream);
+            launched++;
+          }
+          base += nsb_of(q);
+        }
+      }
+      j = k + 1;
+    }
     return launched;
   }
 
@@ -780,8 +818,13 @@ struct celv2_engine {
     free_graphs();  // they hold the old buffers' addresses
     group_jobs = 0;  // the last group's records go with the old host buffer
     for (JobBuffers& b : group) free_buffers(b);
+    cudaFree(group_feats);
+    group_feats = nullptr;
     group.assign(frames, JobBuffers{});
     for (JobBuffers& b : group) alloc_buffers(b, true);
+    const size_t per = (size_t)g.nsb * CELV2_PRUNER_FEATURES;
+    CK(cudaMalloc(&group_feats, per * frames * sizeof(float)));
+    for (int j = 0; j < frames; j++) group[j].feats = group_feats + per * j;
     if (group_host) CK(cudaFreeHost(group_host));
     CK(cudaMallocHost(&group_host, (size_t)frames * g.nsb * sizeof(celv2_sb_out)));
     group_cap = frames;
@@ -1323,12 +1366,13 @@ int celv2_set_pruner(celv2_engine* e, const float* params, float ref_threshold, 
     e->free_graphs();  // captured batches hold the old settings
     if (!params) {
       cudaFree(e->pruner_params), cudaFree(e->nn_acts);
-      e->pruner_params = nullptr, e->nn_acts = nullptr;
+      e->pruner_params = nullptr, e->nn_acts = nullptr, e->nn_cap = 0;
       return;
     }
     if (!e->pruner_params) {
+      e->nn_cap = std::max<long long>(e->g.nsb, 2048);  // a 10-frame 1080p group in three chunks
       CK(cudaMalloc(&e->pruner_params, CELV2_PRUNER_PARAMS * sizeof(float)));
-      CK(cudaMalloc(&e->nn_acts, (size_t)e->g.nsb * CELV2_PRUNER_ACTS * sizeof(float)));
+      CK(cudaMalloc(&e->nn_acts, (size_t)e->nn_cap * CELV2_PRUNER_ACTS * sizeof(float)));
     }
     CK(cudaMemcpy(e->pruner_params, params, CELV2_PRUNER_PARAMS * sizeof(float), cudaMemcpyHostToDevice));
     e->pruner_tr = ref_threshold, e->pruner_ti = intra_threshold, e->pruner_band = band;

@@ -194,6 +194,11 @@ __global__ void k_concat(const float* __restrict__ a3, const float* __restrict__
   }
 }
 
+__global__ void k_relu(float* a, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    a[i] = fmaxf(a[i], 0.f);
+}
+
 // dz = da where the activation is positive (ReLU backward; in place allowed)
 __global__ void k_relu_bwd(const float* __restrict__ act, const float* da, float* dz, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
@@ -253,7 +258,10 @@ void forward(const float* P, const float* x, int batch, float* acts, cudaStream_
   k_im2col<<<grid_for(b * kCols3), 256, 0, st>>>(c.a2, kA2, 8, 8, 32, 2, c.cols3, b * kCols3);
   gemm((int)(b * 16), 32, 288, c.cols3, 288, 1, P + kW3, 1, 288, c.a3, 32, 1, P + kB3, true, false, st);
   k_concat<<<grid_for(b * kH0), 256, 0, st>>>(c.a3, x, c.h0, b * kH0);
-  gemm(batch, 64, 632, c.h0, 632, 1, P + kW4, 1, 632, c.a4, 64, 1, P + kB4, true, false, st);
+  // the dense layer's K (632) in 8 slices on separate CTAs (few rows, many columns of K), then ReLU
+  cudaMemsetAsync(c.a4, 0, (size_t)b * kA4 * sizeof(float), st);
+  gemm(batch, 64, 632, c.h0, 632, 1, P + kW4, 1, 632, c.a4, 64, 1, P + kB4, false, false, st, 8);
+  k_relu<<<grid_for(b * kA4), 256, 0, st>>>(c.a4, b * kA4);
   gemm(batch, 8, 64, c.a4, 64, 1, P + kW5, 1, 64, c.logits, 8, 1, P + kB5, false, false, st);
 }
 

@@ -79,8 +79,8 @@ def mask_costs(eng: E.CudaEngine, clip, qindex: int, plan=None):
     are searched exactly as without pruning), so deciding each frame once per mask -- the same mask
     for all its superblocks -- gives every superblock's cost for every mask. Returns
     (features {frame: nsb x FEATURES}, costs {frame: nsb x 2^(nrefs + 1) int64}, nrefs {frame}); mask
-    index m keeps the references of its low nrefs bits (none: entry unused, set to the full cost)
-    and intra if bit nrefs is set."""
+    index m keeps the references of its low nrefs bits (none named: all of them, as celv2_set_keep
+    reads it) and intra if bit nrefs is set."""
     plan = plan or gop.mini_gop_plan(len(clip))
     eng.clear_store()
     for i, f in enumerate(clip):
@@ -101,8 +101,9 @@ def mask_costs(eng: E.CudaEngine, clip, qindex: int, plan=None):
         eng.set_config(E.CFG_FEATURES, 0)
         top = max(2 ** (len(r) + 1) for _, r in jobs)
         for m in range(top - 1):
+            # m == 2^n names no reference and keeps intra: the full search, measured above
             live = [(j, s, refs) for j, (s, refs) in enumerate(jobs)
-                    if m < 2 ** (len(refs) + 1) - 1 and m & ((1 << len(refs)) - 1)]
+                    if m < 2 ** (len(refs) + 1) - 1 and m != 2 ** len(refs)]
             if not live:
                 continue
             for k, (_, s, refs) in enumerate(live):
@@ -112,10 +113,7 @@ def mask_costs(eng: E.CudaEngine, clip, qindex: int, plan=None):
             for k, (_, s, _) in enumerate(live):
                 costs[s][:, m] = eng.sb_costs(k)
         for s, refs in jobs:
-            n = len(refs)
-            for m in range(2 ** (n + 1)):
-                if not m & ((1 << n) - 1):
-                    costs[s][:, m] = costs[s][:, -1]
+            costs[s][:, 2 ** len(refs)] = costs[s][:, -1]
     return feats, costs, nrefs
 
 
@@ -148,6 +146,7 @@ def policy_labels(keeps: dict, nrefs: dict):
     for s, k in keeps.items():
         n = nrefs[s]
         bits = np.unpackbits(k[:, None], axis=1, bitorder="little").astype(np.float32)
+        bits[bits[:, :n].sum(1) == 0, :n] = 1.0  # no reference named: all of them
         y = np.zeros((k.size, 8), np.float32)
         y[:, :n] = bits[:, :n]
         y[:, 7] = bits[:, 7]

@@ -113,8 +113,10 @@ def main():
                     costs, ms, kept = V.run(eng, plan, 130, reps=3)
                     eng.set_pruner(None)
                 elif s[0] == "exact":
-                    keeps = D.policy(tables[i][1], tables[i][2], mu)[0]
+                    keeps, _, predicted = D.policy(tables[i][1], tables[i][2], mu)
                     costs, ms, kept = V.run(eng, plan, 130, masks=lambda f, n, nsb, k=keeps: k[f], reps=3)
+                    rows.append({"setting": ["exact-predicted"], "loss": predicted, "speedup": 0.0, "ms": 0.0,
+                                 "ms_full": ms_full, "refs_kept": 0.0, "intra_kept": 0.0})
                 else:
                     costs, ms, kept = V.run(eng, plan, 130, masks=V.nearest(s[1], s[2]), reps=3)
                 rows.append({"setting": list(s), "loss": V.cost_increase(costs, full), "speedup": ms_full / ms,

@@ -163,3 +163,28 @@ def test_engine_applies_the_networks_masks(oracle):
     want_rec, want_cost = oracle.decide_masked(w, h, src, refs, lam.lambda_q8(120), masks)
     assert records_equal(got.records, want_rec), first_difference(got.records, want_rec)
     assert (costs == want_cost).all()
+
+
+def test_group_runs_one_network_pass(oracle):
+    """A group's jobs share one batched network pass (their features are consecutive rows); each
+    job's records are the oracle's for the masks the pass chose, also across cache chunks."""
+    from celv2_b200 import synth
+
+    w, h = 416, 240
+    clip = synth.small_clip(seed=17, frames=6)
+    p, _ = case(1, seed=5)
+    jobs = [(5, [4, 3, 2, 1]), (4, [3, 2]), (3, []), (2, [1, 0])]
+    with E.CudaEngine(w, h) as e:
+        for i, f in enumerate(clip):
+            e.upload(f.hy, i)
+        e.set_pruner(p, 0.5, 0.5, 0.0)
+        for graphs in (0, 1):
+            e.set_config(E.CFG_GRAPHS, graphs)
+            e.launch_group([s for s, _ in jobs], [r for _, r in jobs], 130, to_host=True)
+            for j, (s, refs) in enumerate(jobs):
+                keep = e.pruner_masks(j) if refs else None
+                want, want_cost = oracle.decide_masked(w, h, clip[s].y, [clip[r].y for r in refs],
+                                                       lam.lambda_q8(130), keep)
+                got = e.group_records(j)
+                assert records_equal(got, want), f"job {j}: {first_difference(got, want)}"
+                assert (e.sb_costs(j) == want_cost).all()
