@@ -290,6 +290,79 @@ def stage_bytes(plan, steps):
     return out
 
 
+PRUNER_FLOPS = 2 * (256 * 16 * 9 + 64 * 32 * 144 + 16 * 32 * 288 + 632 * 64 + 64 * 8)  # per superblock
+
+
+def run_pruned(eng, plan, args, stream, dist, local, world, plain_value):
+    """The learned-pruned engine (celv2_set_pruner with the committed weights and thresholds) on
+    the same mini-GOP: frames/s timed like `value`, its speed-up, and what it costs -- the summed
+    cost of the chosen partitions over the inter frames against the exhaustive search's (the engine's
+    own rate-distortion measure; BD-rate needs AVM) -- with the share of options it kept."""
+    import numpy as np
+    import torch
+
+    from celv2_b200 import pruner
+
+    if not os.path.exists(pruner.WEIGHTS):
+        return {"unavailable": "no trained weights (python -m celv2_b200.pruner.train)"}
+    wts = pruner.load()
+    nsb = eng.sb_cols * eng.sb_rows
+
+    def costs_pass(masks: bool):
+        costs, kept = {}, {}
+        for group in plan:
+            eng.launch_group([s for s, _ in group], [r for _, r in group], QINDEX)
+            for j, (s, refs) in enumerate(group):
+                if refs:
+                    costs[s] = eng.sb_costs(j)
+                    if masks:
+                        kept[s] = (eng.pruner_masks(j), len(refs))
+        return costs, kept
+
+    full, _ = costs_pass(False)
+    eng.set_pruner(wts["params"], wts["ref_threshold"], wts["intra_threshold"], wts["band"])
+    try:
+        pruned, kept = costs_pass(True)
+        for group in plan * max(1, args.warmup):
+            eng.launch_group([s for s, _ in group], [r for _, r in group], QINDEX)
+        eng.finish()
+        barrier(dist, local)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(local)
+        a.record(stream)
+        for _ in range(args.steps):
+            for group in plan:
+                eng.launch_group([s for s, _ in group], [r for _, r in group], QINDEX)
+        b.record(stream)
+        b.synchronize()
+        ms = max_over_ranks(a.elapsed_time(b), dist, local)
+        eng.stage_timing(True)
+        eng.stage_times()
+        for group in plan:
+            eng.launch_group([s for s, _ in group], [r for _, r in group], QINDEX)
+        st = eng.stage_times()
+        eng.stage_timing(False)
+    finally:
+        eng.set_pruner(None)
+    value = NFRAMES * args.steps * world / (ms / 1e3)
+    loss = sum(float(v.sum()) for v in pruned.values()) / sum(float(full[k].sum()) for k in pruned) - 1.0
+    refs = sum(int(np.unpackbits(k[:, None], axis=1, bitorder="little")[:, :n].sum()) for k, n in kept.values())
+    refs_all = sum(n * nsb for _, n in kept.values())
+    intra = sum(int((k >> 7).sum()) for k, _ in kept.values()) / (nsb * len(kept))
+    net_ms = st["pruner"][0]
+    inter_sbs = nsb * sum(1 for g in plan for _, r in g if r)
+    return {"value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "speedup_vs_plain": value / plain_value,
+            "rd_cost_increase": loss, "refs_kept": refs / refs_all, "intra_kept": intra,
+            "bd_rate": "unavailable: needs the AVM v1.0.0 encoder and decoder (not in this image)",
+            "thresholds": {"ref": wts["ref_threshold"], "intra": wts["intra_threshold"], "band": wts["band"]},
+            "stages_ms_per_step": {k: v[0] for k, v in st.items() if v[1]},
+            "network": {"ms_per_step": net_ms, "superblocks_per_step": inter_sbs,
+                        "bf16_tflops": PRUNER_FLOPS * inter_sbs / (net_ms / 1e3) / 1e12 if net_ms else None,
+                        "note": "features, BF16 tensor-core forward pass (mma.sync) and masks, per step"},
+            "quality_measure": "summed chosen-partition cost (lambda-weighted SATD + rate, the engine's own RD "
+                               "measure) over the inter frames, pruned / exhaustive - 1"}
+
+
 def run_e2e(eng, clip, plan, steps, dist, local, world):
     """Frames/s end to end through the public API, wall clock around whole steps, max over ranks.
     Every step uploads its 17 frames from host 10-bit planes (new keys: new pictures) and brings
@@ -415,6 +488,9 @@ def run_cuda_arm(args):
     dominant = max(st, key=lambda k: st[k][0])
     dom_ms, dom_n = st[dominant]
 
+    # the learned-pruned engine on the same workload (the metric's second half)
+    pruned = None if args.no_pruned else run_pruned(eng, plan, args, stream, dist, local, world, value)
+
     # e2e: host 10-bit planes in, decision records back in host memory, every step
     e2e = run_e2e(eng, clip, plan, max(1, min(args.steps, 5)), dist, local, world)
 
@@ -465,7 +541,7 @@ def run_cuda_arm(args):
                                       "tuned": {k: v for k, v in (tuned or {}).items() if k != "stage_ms"}}},
                 "clocks": clocks.summary(), "gpu_launches": launches,
                 "e2e": e2e,
-                "roofline": roofline, "cpu_baseline": cpu}
+                "roofline": roofline, "cpu_baseline": cpu, "pruned": pruned}
         print(json.dumps(line))
     eng.close()
     if dist is not None:
@@ -497,6 +573,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-pruned", action="store_true", help="skip the learned-pruned variant")
     ap.add_argument("--no-tune", action="store_true", help="default launch configuration")
     ap.add_argument("--no-graphs", action="store_true", help="stage-by-stage launches instead of CUDA graphs")
     ap.add_argument("--profile", action="store_true", help="the small case for ncu captures")

@@ -179,14 +179,12 @@ enum StageId { kStUpload, kStPhases, kStMe4, kStMe3, kStMe2, kStMe1, kStMe0, kSt
                kStPruner, kStages };
 
 // A job's learned-pruner work, queued between motion-search levels 1 and 0: its features into
-// `feats` (when non-null), and with `net` the network's forward pass (cache `acts`) and the masks
-// into `keep`.
+// `feats` (when non-null), and with `net` the network and the masks into `keep`.
 struct NetJob {
   float* feats = nullptr;
   bool net = false;
   const float* params = nullptr;
-  float* acts = nullptr;
-  long long cap = 0;  // samples `acts` holds
+  const void* wb = nullptr;  // bf16 weight copies of the inference kernel
   uint8_t* keep = nullptr;
   float tr = 0, ti = 0, band = 0;
 };
@@ -274,8 +272,7 @@ struct celv2_engine {
   // the learned pruner: features on request, the network when parameters are set
   bool features_on = false;
   float* pruner_params = nullptr;  // device, CELV2_PRUNER_PARAMS floats
-  float* nn_acts = nullptr;        // device, nn_cap x CELV2_PRUNER_ACTS floats
-  long long nn_cap = 0;
+  void* nn_wb = nullptr;           // device, bf16 weight copies for the inference kernel
   float pruner_tr = 0.5f, pruner_ti = 0.5f, pruner_band = 0.f;
 
   // The pruner work of a job of this engine (buffers b; keep_given: celv2_set_keep masks win).
@@ -284,7 +281,7 @@ struct celv2_engine {
     if (job.nrefs == 0) return n;
     const bool net = pruner_params && !keep_given;
     if (!features_on && !net) return n;
-    n.feats = b.feats, n.net = net, n.params = pruner_params, n.acts = nn_acts, n.cap = nn_cap, n.keep = b.keep;
+    n.feats = b.feats, n.net = net, n.params = pruner_params, n.wb = nn_wb, n.keep = b.keep;
     n.tr = pruner_tr, n.ti = pruner_ti, n.band = pruner_band;
     return n;
   }
@@ -346,7 +343,7 @@ struct celv2_engine {
     cudaFree(stats);
     cudaFree(queues);
     cudaFree(pruner_params);
-    cudaFree(nn_acts);
+    cudaFree(nn_wb);
     cudaFree(group_feats);
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     cudaFree(djobs);
@@ -626,44 +623,21 @@ struct celv2_engine {
     return launched;
   }
 
-  // The pruner's features per job, then its network over runs of consecutive jobs whose features
-  // are consecutive rows (a group's slots) and that share parameters, in chunks of the cache's
-  // capacity, then each job's masks; returns the kernels launched.
+  // The pruner's features per job, then per job one kernel running the network on each
+  // superblock and writing its mask; returns the kernels launched.
   int enqueue_pruner(const std::vector<FrameJob>& jobs, const std::vector<NetJob>& nets, cudaStream_t stream) {
     const int n = std::min((int)jobs.size(), (int)nets.size());
-    const long long F = CELV2_PRUNER_FEATURES;
     int launched = 0;
-    auto nsb_of = [&](int j) { return (long long)jobs[j].sb_cols * jobs[j].sb_rows; };
-    for (int j = 0; j < n; j++)
-      if (nets[j].feats) launch_features(djobs + j, (int)nsb_of(j), nets[j].feats, stream), launched++;
-    for (int j = 0; j < n;) {
-      if (!nets[j].net) {
-        j++;
-        continue;
+    for (int j = 0; j < n; j++) {
+      const NetJob& nj = nets[j];
+      if (!nj.feats) continue;
+      const int nsb = jobs[j].sb_cols * jobs[j].sb_rows;
+      launch_features(djobs + j, nsb, nj.feats, stream);
+      launched++;
+      if (nj.net) {
+        launch_infer(nj.params, nj.wb, nj.feats, nsb, jobs[j].nrefs, nj.tr, nj.ti, nj.band, nj.keep, stream);
+        launched++;
       }
-      const NetJob& a = nets[j];
-      int k = j;
-      long long rows = nsb_of(j);
-      while (k + 1 < n && nets[k + 1].net && nets[k + 1].params == a.params && nets[k + 1].acts == a.acts &&
-             nets[k + 1].feats == nets[k].feats + nsb_of(k) * F)
-        rows += nsb_of(++k);
-      for (long long r0 = 0; r0 < rows; r0 += a.cap) {
-        const int cb = (int)std::min(a.cap, rows - r0);
-        pruner_forward(a.params, a.feats + r0 * F, cb, a.acts, stream);
-        launched += 12;
-        const float* logits = a.acts + (long long)cb * (CELV2_PRUNER_ACTS - CELV2_PRUNER_OUTPUTS);
-        long long base = 0;
-        for (int q = j; q <= k; q++) {
-          const long long lo = std::max(base, r0), hi = std::min(base + nsb_of(q), r0 + cb);
-          if (lo < hi) {
-            launch_masks(logits + (lo - r0) * CELV2_PRUNER_OUTPUTS, (int)(hi - lo), jobs[q].nrefs, nets[q].tr,
-                         nets[q].ti, nets[q].band, nets[q].keep + (lo - base), stream);
-            launched++;
-          }
-          base += nsb_of(q);
-        }
-      }
-      j = k + 1;
     }
     return launched;
   }
@@ -1365,16 +1339,17 @@ int celv2_set_pruner(celv2_engine* e, const float* params, float ref_threshold, 
     e->wait_idle();
     e->free_graphs();  // captured batches hold the old settings
     if (!params) {
-      cudaFree(e->pruner_params), cudaFree(e->nn_acts);
-      e->pruner_params = nullptr, e->nn_acts = nullptr, e->nn_cap = 0;
+      cudaFree(e->pruner_params), cudaFree(e->nn_wb);
+      e->pruner_params = nullptr, e->nn_wb = nullptr;
       return;
     }
     if (!e->pruner_params) {
-      e->nn_cap = std::max<long long>(e->g.nsb, 2048);  // a 10-frame 1080p group in three chunks
       CK(cudaMalloc(&e->pruner_params, CELV2_PRUNER_PARAMS * sizeof(float)));
-      CK(cudaMalloc(&e->nn_acts, (size_t)e->nn_cap * CELV2_PRUNER_ACTS * sizeof(float)));
+      CK(cudaMalloc(&e->nn_wb, infer_weight_elems() * 2));
     }
     CK(cudaMemcpy(e->pruner_params, params, CELV2_PRUNER_PARAMS * sizeof(float), cudaMemcpyHostToDevice));
+    infer_weights(e->pruner_params, e->nn_wb, e->st);
+    CK(cudaStreamSynchronize(e->st));
     e->pruner_tr = ref_threshold, e->pruner_ti = intra_threshold, e->pruner_band = band;
   });
 }

@@ -78,6 +78,12 @@ void launch_features(const FrameJob* djob, int nsb, float* out, cudaStream_t st)
 void pruner_forward(const float* params, const float* x, int batch, float* acts, cudaStream_t st);
 void launch_masks(const float* logits, int nsb, int nrefs, float tr, float ti, float band, uint8_t* keep,
                   cudaStream_t st);
+// The engine's inference: the network and the mask of every superblock of one job in one kernel,
+// from bf16 weight copies (infer_weights: infer_weight_elems() bf16 elements).
+size_t infer_weight_elems();
+void infer_weights(const float* params, void* wb, cudaStream_t st);
+void launch_infer(const float* params, const void* wb, const float* feats, int nsb, int nrefs, float tr, float ti,
+                  float band, uint8_t* keep, cudaStream_t st);
 
 // Set-up of the constant tables (once per device).
 cudaError_t init_tables();

@@ -383,6 +383,162 @@ void pruner_forward(const float* params, const float* x, int batch, float* acts,
   nn::forward(params, x, batch, acts, st);
 }
 
+// ---- the engine's inference: the whole network for one superblock per CTA, then its mask ----
+// The same arithmetic as nn::forward (BF16 operands, FP32 sums; only the order of the sums
+// differs): the 3x3 convolution 1 -> 16 and the dense layers on the CUDA cores (bf16-rounded
+// operands), the two strided convolutions (85% of the FLOPs) as mma.sync m16n8k16 tiles whose A
+// operand is read straight from the previous activation in shared memory (an implicit im2col).
+// Weights: bf16 copies made once (infer_weights), W4 transposed so a CTA's 64 threads read rows.
+namespace nn {
+constexpr int kIW2 = 0, kIW3 = kIW2 + 32 * 144, kIW4 = kIW3 + 32 * 288, kIWs = kIW4 + 632 * 64;  // bf16 elements
+
+__global__ void k_infer_weights(const float* __restrict__ P, __nv_bfloat16* __restrict__ Wb) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kIWs; i += gridDim.x * blockDim.x) {
+    float v;
+    if (i < kIW3) v = P[kW2 + i];
+    else if (i < kIW4) v = P[kW3 + (i - kIW3)];
+    else {
+      const int r = i - kIW4, k = r / 64, o = r - k * 64;  // W4t[k][o] = W4[o][k]
+      v = P[kW4 + o * 632 + k];
+    }
+    Wb[i] = __float2bfloat16_rn(v);
+  }
+}
+
+__device__ __forceinline__ float rbf(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+
+__device__ __forceinline__ void mma16816(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__global__ void __launch_bounds__(128) k_infer(const float* __restrict__ P, const __nv_bfloat16* __restrict__ Wb,
+                                               const float* __restrict__ feats, int nrefs, float tr, float ti,
+                                               float band, uint8_t* __restrict__ keep) {
+  __shared__ float xr[kF];                            // the features, bf16-rounded
+  __shared__ __align__(16) __nv_bfloat16 a1[256][16];  // conv1 output, (y, x) rows, channels
+  __shared__ __align__(16) __nv_bfloat16 a2[64][32];
+  __shared__ float h0[632], a4[64], part[128];
+  __shared__ float logits[kOut];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t = lane & 3;
+  const float* x = feats + (long long)blockIdx.x * kF;
+  for (int i = tid; i < kF; i += 128) xr[i] = rbf(x[i]);
+  __syncthreads();
+  // conv 3x3 1 -> 16, stride 1
+  for (int e = tid; e < 256 * 16; e += 128) {
+    const int p = e >> 4, c = e & 15, y = p >> 4, xx = p & 15;
+    float s = 0.f;
+#pragma unroll
+    for (int ky = 0; ky < 3; ky++)
+#pragma unroll
+      for (int kx = 0; kx < 3; kx++) {
+        const int iy = y + ky - 1, ix = xx + kx - 1;
+        if (iy >= 0 && iy < 16 && ix >= 0 && ix < 16) s += xr[iy * 16 + ix] * rbf(P[kW1 + c * 9 + ky * 3 + kx]);
+      }
+    a1[p][c] = __float2bfloat16_rn(fmaxf(s + P[kB1 + c], 0.f));
+  }
+  __syncthreads();
+  // conv 3x3 16 -> 32, stride 2: rows = 64 output positions (warp w: 16w..16w+15), K = tap x 16
+  {
+    float acc[4][4] = {};
+    const int r0 = warp * 16 + g, r1 = r0 + 8;
+    for (int tap = 0; tap < 9; tap++) {
+      const int ky = tap / 3, kx = tap - ky * 3;
+      uint32_t a[4];
+      const int iy0 = (r0 >> 3) * 2 + ky - 1, ix0 = (r0 & 7) * 2 + kx - 1;
+      const int iy1 = (r1 >> 3) * 2 + ky - 1, ix1 = (r1 & 7) * 2 + kx - 1;
+      const bool in0 = iy0 >= 0 && iy0 < 16 && ix0 >= 0 && ix0 < 16, in1 = iy1 >= 0 && iy1 < 16 && ix1 >= 0 && ix1 < 16;
+      const uint32_t* q0 = reinterpret_cast<const uint32_t*>(a1[in0 ? iy0 * 16 + ix0 : 0]);
+      const uint32_t* q1 = reinterpret_cast<const uint32_t*>(a1[in1 ? iy1 * 16 + ix1 : 0]);
+      a[0] = in0 ? q0[t] : 0u, a[1] = in1 ? q1[t] : 0u, a[2] = in0 ? q0[t + 4] : 0u, a[3] = in1 ? q1[t + 4] : 0u;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(Wb + kIW2 + (j * 8 + g) * 144 + tap * 16);
+        mma16816(acc[j], a, __ldg(w + t), __ldg(w + t + 4));
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = q < 2 ? r0 : r1, n = j * 8 + 2 * t + (q & 1);
+        a2[r][n] = __float2bfloat16_rn(fmaxf(acc[j][q] + P[kB2 + n], 0.f));
+      }
+  }
+  __syncthreads();
+  // conv 3x3 32 -> 32, stride 2: 16 output positions, warp w: output channels 8w..8w+7, K = tap x 32
+  {
+    float acc[4] = {};
+    const int r0 = g, r1 = g + 8;
+    for (int s = 0; s < 18; s++) {
+      const int tap = s >> 1, c0 = (s & 1) * 16, ky = tap / 3, kx = tap - ky * 3;
+      uint32_t a[4];
+      const int iy0 = (r0 >> 2) * 2 + ky - 1, ix0 = (r0 & 3) * 2 + kx - 1;
+      const int iy1 = (r1 >> 2) * 2 + ky - 1, ix1 = (r1 & 3) * 2 + kx - 1;
+      const bool in0 = iy0 >= 0 && iy0 < 8 && ix0 >= 0 && ix0 < 8, in1 = iy1 >= 0 && iy1 < 8 && ix1 >= 0 && ix1 < 8;
+      const uint32_t* q0 = reinterpret_cast<const uint32_t*>(&a2[in0 ? iy0 * 8 + ix0 : 0][c0]);
+      const uint32_t* q1 = reinterpret_cast<const uint32_t*>(&a2[in1 ? iy1 * 8 + ix1 : 0][c0]);
+      a[0] = in0 ? q0[t] : 0u, a[1] = in1 ? q1[t] : 0u, a[2] = in0 ? q0[t + 4] : 0u, a[3] = in1 ? q1[t + 4] : 0u;
+      const uint32_t* w = reinterpret_cast<const uint32_t*>(Wb + kIW3 + (warp * 8 + g) * 288 + tap * 32 + c0);
+      mma16816(acc, a, __ldg(w + t), __ldg(w + t + 4));
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int r = q < 2 ? r0 : r1, n = warp * 8 + 2 * t + (q & 1);
+      h0[r * 32 + n] = rbf(fmaxf(acc[q] + P[kB3 + n], 0.f));  // the dense layer reads it as BF16
+    }
+  }
+  for (int i = tid; i < 120; i += 128) h0[512 + i] = xr[256 + i];
+  __syncthreads();
+  // dense 632 -> 64: thread (o, half) sums half of the row
+  {
+    const int o = tid & 63, half = tid >> 6;
+    float s = 0.f;
+    for (int k = half * 316; k < half * 316 + 316; k++) s += h0[k] * __bfloat162float(Wb[kIW4 + k * 64 + o]);
+    part[tid] = s;
+  }
+  __syncthreads();
+  if (tid < 64) a4[tid] = rbf(fmaxf(part[tid] + part[tid + 64] + P[kB4 + tid], 0.f));
+  __syncthreads();
+  // dense 64 -> 8: warp w, lanes sum over the 64 inputs for outputs 2w, 2w + 1
+  for (int o = warp * 2; o < warp * 2 + 2; o++) {
+    float s = a4[lane] * rbf(P[kW5 + o * 64 + lane]) + a4[lane + 32] * rbf(P[kW5 + o * 64 + lane + 32]);
+    for (int d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
+    if (lane == 0) logits[o] = s + P[kB5 + o];
+  }
+  __syncthreads();
+  if (tid == 0) {  // the mask (k_masks' rule)
+    unsigned k = 0;
+    int best = 0;
+    float pbest = -1.f;
+    bool unsure = false;
+    for (int r = 0; r < nrefs; r++) {
+      const float pr = 1.f / (1.f + expf(-logits[r]));
+      if (pr >= tr) k |= 1u << r;
+      if (pr > pbest) pbest = pr, best = r;
+      unsure |= fabsf(pr - tr) < band;
+    }
+    const float pi = 1.f / (1.f + expf(-logits[7]));
+    if (pi >= ti) k |= 0x80u;
+    unsure |= fabsf(pi - ti) < band;
+    k |= 1u << best;
+    keep[blockIdx.x] = (uint8_t)(unsure ? 0xFFu : k);
+  }
+}
+}  // namespace nn
+
+// bf16 copies of the convolution and dense weights the inference kernel reads (nn::kIWs elements)
+size_t infer_weight_elems() { return nn::kIWs; }
+void infer_weights(const float* params, void* wb, cudaStream_t st) {
+  nn::k_infer_weights<<<nn::grid_for(nn::kIWs), 256, 0, st>>>(params, static_cast<__nv_bfloat16*>(wb));
+}
+void launch_infer(const float* params, const void* wb, const float* feats, int nsb, int nrefs, float tr, float ti,
+                  float band, uint8_t* keep, cudaStream_t st) {
+  nn::k_infer<<<nsb, 128, 0, st>>>(params, static_cast<const __nv_bfloat16*>(wb), feats, nrefs, tr, ti, band, keep);
+}
+
 }  // namespace celv2cu
 
 using namespace celv2cu;

@@ -166,8 +166,8 @@ def test_engine_applies_the_networks_masks(oracle):
 
 
 def test_group_runs_one_network_pass(oracle):
-    """A group's jobs share one batched network pass (their features are consecutive rows); each
-    job's records are the oracle's for the masks the pass chose, also across cache chunks."""
+    """In a group every inter job gets the network's masks, with or without graph replay; each job's
+    records are the oracle's for those masks."""
     from celv2_b200 import synth
 
     w, h = 416, 240
