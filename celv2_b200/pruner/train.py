@@ -2,7 +2,7 @@
 
     python -m celv2_b200.pruner.train [--out DIR] [--steps N]
 
-1. seeded synthetic 1080p clips (the workload's generator, other seeds): 12 for training, 2 for
+1. seeded synthetic 1080p clips (the workload's generator, other seeds): 24 for training, 2 for
    choosing the thresholds, 2 held out for the report; qindex 100 / 130 / 160 / 190 in training,
    130 for validation and test (the benchmark's);
 2. for every inter frame, every superblock's chosen cost under every mask (data.mask_costs: a
@@ -29,7 +29,7 @@ from . import data as D
 from . import evaluate as V
 from . import net as N
 
-TRAIN_SEEDS = list(range(101, 113))
+TRAIN_SEEDS = list(range(101, 125))
 VAL_SEEDS = [201, 202]
 TEST_SEEDS = [301, 302]
 QS = [100, 130, 160, 190]
@@ -69,10 +69,11 @@ def main():
     eng.reserve_group(10)
     eng.set_config(E.CFG_GRAPHS, 1)
     plan = V.default_plan()
-    qs = [QS[i % 4] for i in range(12)] + [130] * 4
+    nt = len(TRAIN_SEEDS)
+    qs = [QS[i % 4] for i in range(nt)] + [130] * 4
     tables = [D.mask_costs(eng, c, q, plan) for c, q in zip(clips, qs)]
     print(f"mask costs {time.time() - t0:.1f}s", flush=True)
-    train_t = tables[:12]
+    train_t = tables[:nt]
     # mu on the training clips: each clip's loss weighs by its share of the summed cost
     tot = [sum(float(c[:, -1].sum()) for c in t[1].values()) for t in train_t]
     mu = find_mu([(t[1], t[2], tc / sum(tot)) for t, tc in zip(train_t, tot)], args.target)
@@ -131,21 +132,27 @@ def main():
                  "intra_kept": float(np.mean([r["intra_kept"] for r in v]))} for k, v in agg.items()]
 
     net_settings = [("net", a, b, 0.0) for a in (0.2, 0.3, 0.4, 0.5, 0.6, 0.7) for b in (0.2, 0.3, 0.4, 0.5, 0.6)]
-    val = sweep([12, 13], net_settings + [("exact",)])
+    val = sweep([nt, nt + 1], net_settings + [("exact",)])
     ok = [r for r in val if r["setting"][0] == "net" and r["loss"] <= args.max_loss]
     best = max(ok, key=lambda r: r["speedup"]) if ok else min((r for r in val if r["setting"][0] == "net"),
                                                               key=lambda r: r["loss"])
     _, tr_, ti, band = best["setting"]
     print("chosen", best, flush=True)
     heur = [("nearest", k, intra) for k in (1, 2, 3, 4) for intra in (True, False)]
-    test = sweep([14, 15], [("net", tr_, ti, band), ("exact",)] + heur)
+    test = sweep([nt + 2, nt + 3], [("net", tr_, ti, band), ("exact",)] + heur)
+    # the exact policy's trade-off on the held-out clips (no network: what perfect masks would give)
+    curve = []
+    for f in (0.25, 0.5, 1.0, 2.0, 4.0, 8.0):
+        pts = [D.policy(tables[i][1], tables[i][2], mu * f) for i in (nt + 2, nt + 3)]
+        curve.append({"mu": mu * f, "loss": float(np.mean([p[2] for p in pts])),
+                      "work_kept": float(np.mean([p[1] for p in pts]))})
     os.makedirs(args.out, exist_ok=True)
     np.savez(os.path.join(args.out, "weights.npz"), params=params, ref_threshold=np.float32(tr_),
              intra_threshold=np.float32(ti), band=np.float32(band))
     report = {"samples": int(X.shape[0]), "steps": args.steps, "batch": args.batch, "loss_curve": losses,
               "mu": mu, "target": args.target, "exact_policy_work": float(np.mean(oracle_work)),
               "targets_positive": (Y.sum(0) / np.maximum(Wt.astype(bool).sum(0), 1)).tolist(),
-              "validation": val, "chosen": best, "test": test,
+              "validation": val, "chosen": best, "test": test, "exact_policy_curve": curve,
               "seeds": {"train": TRAIN_SEEDS, "val": VAL_SEEDS, "test": TEST_SEEDS}, "seconds": time.time() - t0}
     with open(os.path.join(args.out, "report.json"), "w") as fh:
         json.dump(report, fh, indent=1)

@@ -188,3 +188,34 @@ def test_group_runs_one_network_pass(oracle):
                 got = e.group_records(j)
                 assert records_equal(got, want), f"job {j}: {first_difference(got, want)}"
                 assert (e.sb_costs(j) == want_cost).all()
+
+
+def test_network_beats_the_heuristic_without_it():
+    """On a held-out 1080p mini-GOP (a seed no training clip used), the committed network at its
+    committed thresholds keeps less work than the best rule without it at that speed (the three
+    nearest references plus intra) and loses less: the summed chosen-partition cost rises less over
+    the exhaustive search."""
+    from celv2_b200 import pruner, synth
+    from celv2_b200.pruner import evaluate as V
+
+    clip = [f.hy for f in synth.hd_clip(301)]
+    wts = pruner.load()
+    plan = V.default_plan()
+    nrefs = np.mean([len(r) for g in plan for _, r in g if r])
+    with E.CudaEngine(1920, 1080) as e:
+        e.reserve_group(10)
+        V.upload(e, clip)
+        full, _, _ = V.run(e, plan, 130)
+        e.set_pruner(wts["params"], wts["ref_threshold"], wts["intra_threshold"], wts["band"])
+        net, _, kept_net = V.run(e, plan, 130)
+        e.set_pruner(None)
+        heur, _, kept_heur = V.run(e, plan, 130, masks=V.nearest(3, True))
+
+    def work(kept):
+        k = V.kept_work(kept, plan)
+        return k["refs_kept"] * nrefs + 1.48 * k["intra_kept"]
+
+    loss_net, loss_heur = V.cost_increase(net, full), V.cost_increase(heur, full)
+    assert work(kept_net) <= work(kept_heur)
+    assert loss_net < loss_heur
+    assert 0.0 <= loss_net < 0.02
