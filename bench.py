@@ -270,8 +270,8 @@ def stage_units(plan, steps):
     """Work units per stage over `steps` steps (the units of profiles/traffic.json)."""
     cells, inter_refs, frames = plan_counts(plan)
     nsb = ((W + 63) // 64) * ((H + 63) // 64)
-    return {"me_l0": cells[0] * steps, "inter": inter_refs * nsb * steps, "intra": frames * nsb * steps,
-            "finalize": frames * nsb * steps}
+    return {"me_l0": cells[0] * steps, "me_refine": cells[0] * steps, "inter": inter_refs * nsb * steps,
+            "intra": frames * nsb * steps, "finalize": frames * nsb * steps}
 
 
 def stage_bytes(plan, steps):
