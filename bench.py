@@ -367,18 +367,28 @@ def run_e2e(eng, clip, plan, steps, dist, local, world):
     """Frames/s end to end through the public API, wall clock around whole steps, max over ranks.
     Every step uploads its 17 frames from host 10-bit planes (new keys: new pictures) and brings
     every record back into host memory.
-      value     -- the mini-GOP through CudaEngine.decide_group (celv2_upload, celv2_set_output,
-                   celv2_launch_group): groups issued back to back, the records copied straight into
-                   the DecisionMaps while the next group runs; the step ends when all are in host
-                   memory.
+      value     -- the mini-GOP through CudaEngine.decide_group (celv2_upload_pinned,
+                   celv2_set_output, celv2_launch_group) from page-locked host planes (a frame pool,
+                   filled once before timing): groups issued back to back, the planes copied by DMA
+                   and the records straight into the DecisionMaps while the next group runs; the step
+                   ends when all are in host memory.
       per_group -- the same, waiting for each group's records before the next group is issued.
+      pageable  -- `value` from ordinary (pageable) numpy planes: celv2_upload copies each into
+                   a staging buffer on the host first.
       per_frame -- the reference's own interface: launch / prepare / collect per frame (celv2_launch,
                    celv2_prepare, celv2_wait_row), every reference uploaded once per step."""
     from celv2_b200 import engine as E
     from celv2_b200.records import DecisionMap
 
+    import numpy as np
+
     nsb = eng.sb_cols * eng.sb_rows
     plane = clip[0].hy.nbytes
+    pool = []  # the page-locked frame pool (an encoder keeps its source frames in one)
+    for f in clip:
+        a = E.host_array(f.hy.shape, np.uint16)
+        a[...] = f.hy
+        pool.append(a)
 
     def timed(run):
         run(0)  # warm: pools, graphs
@@ -391,13 +401,15 @@ def run_e2e(eng, clip, plan, steps, dist, local, world):
         dt = max_over_ranks(time.perf_counter() - t0, dist, local)
         return NFRAMES * steps * world / dt
 
-    def groups(s, wait):
+    def groups(s, wait, pinned=True):
         key = lambda d: s * 1000 + d  # noqa: E731 -- new pictures every step (reconstructions differ)
+        planes = pool if pinned else [f.hy for f in clip]
         maps = []
         for group in plan:
-            maps += eng.decide_group([clip[src].hy for src, _ in group],
-                                     [[clip[r].hy for r in refs] for _, refs in group], QINDEX,
-                                     ref_keys=[[key(r) for r in refs] for _, refs in group], wait=wait)
+            maps += eng.decide_group([planes[src] for src, _ in group],
+                                     [[planes[r] for r in refs] for _, refs in group], QINDEX,
+                                     ref_keys=[[key(r) for r in refs] for _, refs in group], wait=wait,
+                                     pinned=pinned)
         return maps
 
     def frames(s):
@@ -419,13 +431,22 @@ def run_e2e(eng, clip, plan, steps, dist, local, world):
 
     pipelined = timed(pipelined_step)
     per_group = timed(lambda s: groups(s, True))
+
+    def pageable_step(s):
+        held.clear()
+        held.extend(groups(s, False, pinned=False))
+        eng.finish()
+
+    pageable = timed(pageable_step)
     per_frame = timed(frames)
     ref_frames = {r for group in plan for _, refs in group for r in refs}
     return {"value": pipelined, "unit": UNIT, "h2d_bytes_per_step": (NFRAMES + len(ref_frames)) * plane,
             "d2h_bytes_per_step": NFRAMES * nsb * RECORD_BYTES, "steps": steps,
-            "api": "CudaEngine.decide_group per coding group (celv2_upload, celv2_set_output, celv2_launch_group); "
-                   "records straight into host DecisionMaps, copies overlapping the next group",
+            "api": "CudaEngine.decide_group per coding group (celv2_upload_pinned, celv2_set_output, "
+                   "celv2_launch_group) from a page-locked frame pool; records straight into host DecisionMaps, "
+                   "copies overlapping the next group",
             "per_group": {"value": per_group, "note": "each group's records in host memory before the next group"},
+            "pageable": {"value": pageable, "note": "the same from pageable numpy planes (celv2_upload)"},
             "per_frame": {"value": per_frame, "h2d_bytes_per_step": (NFRAMES + len(ref_frames)) * plane,
                           "api": "launch/prepare/collect per frame (celv2_launch, celv2_prepare, celv2_wait_row)"}}
 

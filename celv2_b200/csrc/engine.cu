@@ -463,7 +463,10 @@ struct celv2_engine {
   // queues its upload, the 8-bit level 0, the pyramid and (phases) the quarter-pel planes.
   // Uploads f into s on `stream`: 8-bit level 0 and pyramid, the phase planes too when `phases`
   // (room for them when `room`).
-  void upload(const celv2_frame* f, Slot& s, bool phases, cudaStream_t stream, bool room = false) {
+  // direct: the plane is page-locked and stays unchanged until the upload ran (DMA from it, no
+  // staging copy on the host).
+  void upload(const celv2_frame* f, Slot& s, bool phases, cudaStream_t stream, bool room = false,
+              bool direct = false) {
     alloc_slot(s, phases || room || s.phases);
     const bool wide = f->y == nullptr;
     const int pitch = f->pitch ? f->pitch : g.pw;
@@ -471,12 +474,16 @@ struct celv2_engine {
     Stage& sg = take_stage(row * g.ph);
     const uint8_t* src = wide ? reinterpret_cast<const uint8_t*>(f->hy) : f->y;
     const size_t spitch = (size_t)pitch * (wide ? 2 : 1);
-    if (spitch == row) {
-      std::memcpy(sg.host, src, row * g.ph);
+    if (direct) {
+      CK(cudaMemcpy2DAsync(sg.dev, row, src, spitch, row, g.ph, cudaMemcpyHostToDevice, stream));
     } else {
-      for (int r = 0; r < g.ph; r++) std::memcpy((uint8_t*)sg.host + r * row, src + r * spitch, row);
+      if (spitch == row) {
+        std::memcpy(sg.host, src, row * g.ph);
+      } else {
+        for (int r = 0; r < g.ph; r++) std::memcpy((uint8_t*)sg.host + r * row, src + r * spitch, row);
+      }
+      CK(cudaMemcpyAsync(sg.dev, sg.host, row * g.ph, cudaMemcpyHostToDevice, stream));
     }
-    CK(cudaMemcpyAsync(sg.dev, sg.host, row * g.ph, cudaMemcpyHostToDevice, stream));
     stage(kStUpload, stream, [&] {
       if (wide)
         launch_expand_u16((const uint16_t*)sg.dev, g.pw, f->bit_depth, s.pyr.lv[0], stream);
@@ -810,7 +817,7 @@ struct celv2_engine {
     return nullptr;
   }
 
-  void upload_store(const celv2_frame* f, long long key) {
+  void upload_store(const celv2_frame* f, long long key, bool direct = false) {
     check_frame(f, "frame");
     if (key < 0) invalid("store keys must be >= 0");
     // No wait for queued work: it runs on this stream, ahead of the upload.
@@ -831,7 +838,7 @@ struct celv2_engine {
     // planes are made by the first launch that uses the frame as a reference
     if (s->use_pending) CK(cudaStreamWaitEvent(up_st, s->last_use, 0));
     s->use_pending = false;
-    upload(f, *s, false, up_st, true);
+    upload(f, *s, false, up_st, true, direct);
     CK(cudaEventRecord(s->ready, up_st));
     s->ready_pending = true;
     s->key = key;
@@ -1189,6 +1196,21 @@ int celv2_upload(celv2_engine* e, const celv2_frame* f, long long key) {
     if (!e) invalid("null engine");
     CK(cudaSetDevice(e->device));
     e->upload_store(f, key);
+  });
+}
+
+int celv2_upload_pinned(celv2_engine* e, const celv2_frame* f, long long key) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    if (!f || (!f->y && !f->hy)) invalid("upload_pinned: no luma plane");
+    CK(cudaSetDevice(e->device));
+    cudaPointerAttributes a{};
+    const void* plane = f->y ? (const void*)f->y : (const void*)f->hy;
+    if (cudaPointerGetAttributes(&a, plane) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+      cudaGetLastError();
+      invalid("upload_pinned: the plane must be page-locked host memory (celv2_host_alloc)");
+    }
+    e->upload_store(f, key, true);
   });
 }
 

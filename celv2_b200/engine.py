@@ -50,6 +50,7 @@ SIGNATURES = {
     "celv2_wait_row": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]),
     "celv2_finish": (C.c_int, [C.c_void_p]),
     "celv2_upload": (C.c_int, [C.c_void_p, C.POINTER(CelvFrame), C.c_longlong]),
+    "celv2_upload_pinned": (C.c_int, [C.c_void_p, C.POINTER(CelvFrame), C.c_longlong]),
     "celv2_launch_group": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_longlong), C.POINTER(C.c_int),
                                      C.POINTER(C.POINTER(C.c_longlong)), C.POINTER(C.c_int64), C.c_int]),
     "celv2_reserve_group": (C.c_int, [C.c_void_p, C.c_int]),
@@ -165,6 +166,19 @@ class _RecordPool:
 
 
 _records = _RecordPool()
+
+
+def host_array(shape, dtype) -> np.ndarray:
+    """A numpy array in page-locked host memory (celv2_host_alloc), freed with its last view: what
+    celv2_upload_pinned and celv2_set_output take."""
+    dt = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dt.itemsize
+    p = C.c_void_p()
+    _check(library().celv2_host_alloc(max(1, nbytes), C.byref(p)))
+    buf = (C.c_uint8 * max(1, nbytes)).from_address(p.value)
+    fin = weakref.finalize(buf, library().celv2_host_free, p.value)
+    fin.atexit = False
+    return np.ctypeslib.as_array(buf)[:nbytes].view(dt).reshape(shape)
 
 
 def _plane_of(f):
@@ -337,10 +351,16 @@ class CudaEngine:
         return self.decide_inter(src, [], qindex)
 
     # ---- device-resident path ----
-    def upload(self, frame, key: int) -> None:
+    def upload(self, frame, key: int, pinned: bool = False) -> None:
+        """celv2_upload; pinned=True: celv2_upload_pinned (the plane from host_array, DMA after
+        return: keep it unchanged until finish())."""
         keep: list = []
         f = make_frame(frame, self.width, self.height, keep)
-        _check(library().celv2_upload(self._h, C.byref(f), key))
+        if pinned:
+            _check(library().celv2_upload_pinned(self._h, C.byref(f), key))
+            self._inflight.extend(keep)
+        else:
+            _check(library().celv2_upload(self._h, C.byref(f), key))
 
     def reserve_group(self, frames: int) -> None:
         _check(library().celv2_reserve_group(self._h, frames))
@@ -434,12 +454,14 @@ class CudaEngine:
 
     _SRC_KEYS, _TMP_KEYS = 1 << 62, 1 << 61  # store keys of decide_group's sources / unkeyed references
 
-    def decide_group(self, srcs, refs, qindex, ref_keys=None, wait: bool = True) -> list[DecisionMap]:
+    def decide_group(self, srcs, refs, qindex, ref_keys=None, wait: bool = True,
+                     pinned: bool = False) -> list[DecisionMap]:
         """Frames decided together, one launch per stage: the leaves of a mini-GOP as the
         reference's Pipeline::code_group (src/pipeline.cpp:328-384) holds them. Job i decides
         srcs[i] against refs[i] (nearest first); ref_keys[i] (optional) are launch's ref_keys, so a
         reference seen before under its key is not uploaded again. The maps equal separate launch /
-        collect calls' maps. Inputs are copied before it returns; with wait=False the records are
+        collect calls' maps. Inputs are copied before it returns (pinned=True: planes from host_array,
+        copied by DMA afterwards -- keep them until finish()); with wait=False the records are
         defined after finish()."""
         n = len(srcs)
         if len(refs) != n or (ref_keys is not None and len(ref_keys) != n):
@@ -454,18 +476,18 @@ class CudaEngine:
                 if k is None:
                     counter += 1
                     k = self._TMP_KEYS | counter
-                    self.upload(f, k)
+                    self.upload(f, k, pinned)
                     tmp.append(k)
                 elif k not in keyed:
                     if k >= self._TMP_KEYS:
                         raise ValueError("decide_group: reference keys must be below 2**61")
-                    self.upload(f, k)
+                    self.upload(f, k, pinned)
                     keyed.add(k)
                 need.add(k)
                 ks.append(k)
             counter += 1
             sk = self._SRC_KEYS | counter
-            self.upload(srcs[i], sk)
+            self.upload(srcs[i], sk, pinned)
             jobs_src.append(sk)
             jobs_refs.append(ks)
         for k in [k for k in keyed if k not in need]:  # keyed references this group does not use

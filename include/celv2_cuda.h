@@ -93,6 +93,10 @@ const char* celv2_last_error(void);
  * stays until celv2_drop_frame / celv2_clear_store: celv2_launch's own cache of references does not
  * evict it. The upload runs behind the queued work. */
 int celv2_upload(celv2_engine* e, const celv2_frame* f, long long key);
+/* celv2_upload from a plane in page-locked host memory (celv2_host_alloc; else CELV2_EINVAL), by
+ * DMA after the call returns, with no copy on the host: the caller keeps the plane unchanged
+ * until the engine is idle (celv2_finish). No counterpart in the reference. */
+int celv2_upload_pinned(celv2_engine* e, const celv2_frame* f, long long key);
 
 /* One batch of frames decided from the frame store: job i decides the frame with key src_keys[i]
  * against the nrefs[i] frames ref_keys[i][0..]. All jobs' stages run as one launch per stage.

@@ -154,3 +154,27 @@ def test_launch_multi_into_maps(oracle):
     finally:
         for e in engines:
             e.close()
+
+
+def test_pinned_uploads_match_oracle(oracle):
+    """celv2_upload_pinned: planes in page-locked memory go to the device by DMA after the call;
+    the decisions are the oracle's; pageable planes are refused."""
+    w, h = 416, 240
+    clip = synth.small_clip(seed=23, frames=4)
+    pool = []
+    for f in clip:
+        a = E.host_array(f.hy.shape, np.uint16)
+        a[...] = f.hy
+        pool.append(a)
+    with E.CudaEngine(w, h) as e:
+        with pytest.raises(RuntimeError):
+            e.upload(clip[0].hy.copy(), 0, pinned=True)
+        groups = [[(0, [])], [(3, [0])], [(1, [0, 3]), (2, [3, 0])]]
+        out = []
+        for g in groups:
+            out.append(e.decide_group([pool[s] for s, _ in g], [[pool[r] for r in refs] for _, refs in g], 120,
+                                      ref_keys=[list(refs) for _, refs in g], wait=False, pinned=True))
+        e.finish()
+        for g, dms in zip(groups, out):
+            for (s, refs), dm in zip(g, dms):
+                check(oracle, w, h, clip, s, refs, 120, dm.records, f"frame {s}")
