@@ -197,7 +197,7 @@ def run_reference_arm(args):
     eng = ref.engine(W, H, threads)
     eng.hold_frames([f.y for f in clip])
     leaves = mini_gop_plan()[-1]
-    steps = min(args.steps, 12)
+    steps = min(args.steps, 8)
     for i in range(min(args.warmup, 1)):
         src, refs = leaves[i % len(leaves)]
         eng.decide_held(src, refs, QINDEX)
@@ -209,7 +209,7 @@ def run_reference_arm(args):
     eng.close()
     fps = steps / dt
     sample = (f"one 7-reference leaf frame of the 1080p mini-GOP per step ({steps} timed steps"
-              f"{', capped at 12' if args.steps > 12 else ''}, {min(args.warmup, 1)} warm-up), "
+              f"{', capped at 8' if args.steps > 8 else ''}, {min(args.warmup, 1)} warm-up), "
               f"8-bit planes held in the engine, {threads} host threads")
     line = {"metric": METRIC, "value": fps, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": dt / steps * 1e3,

@@ -51,7 +51,7 @@ __device__ __forceinline__ int exact_div(int n, int d, float rcp) {
   return q;
 }
 
-__global__ void __launch_bounds__(kIntraThreads, 3) k_intra(const FrameJob* __restrict__ jobs, WorkList w) {
+__global__ void __launch_bounds__(kIntraThreads, 4) k_intra(const FrameJob* __restrict__ jobs, WorkList w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   IntraSmem& S = *reinterpret_cast<IntraSmem*>(smem_raw);
   __shared__ int unit_slot;
