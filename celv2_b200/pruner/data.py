@@ -155,3 +155,44 @@ def policy_labels(keeps: dict, nrefs: dict):
         w[:, 7] = 1.0
         ys.append(y), ws.append(w)
     return np.concatenate(ys), np.concatenate(ws)
+
+
+def regret_targets(costs: dict, nrefs: dict, mu: float, c_ref: float = 1.0, c_intra: float = 1.48,
+                   floor: float = 0.05):
+    """Cost-sensitive targets: the policy's mask bits, each weighted by the regret of flipping it --
+    how much work + mu * cost increase the superblock loses if that one bit of its optimal mask is
+    wrong -- so the network learns hardest where a mistake is expensive. Weights are scaled to mean
+    1 over the present outputs, plus `floor`; absent references weigh 0."""
+    total = sum(float(c[:, -1].sum()) for c in costs.values())
+    ys, ws = [], []
+    for s, c in costs.items():
+        n = nrefs[s]
+        ms = np.arange(c.shape[1])
+        refbits = ms & ((1 << n) - 1)
+        cnt = np.array([bin(int(r)).count("1") if r else n for r in refbits], np.float64)
+        w = c_ref * cnt + c_intra * ((ms >> n) & 1)
+        obj = w[None, :] + mu * (c - c[:, -1:]).astype(np.float64) / total
+        best = np.argmin(obj, axis=1)
+        rows = np.arange(c.shape[0])
+        y = np.zeros((c.shape[0], 8), np.float32)
+        wt = np.zeros((c.shape[0], 8), np.float32)
+        rb = refbits[best]
+        all_refs = rb == 0  # no reference named: all of them
+        for r in range(n):
+            y[:, r] = np.where(all_refs, 1.0, (rb >> r) & 1)
+            flip = best ^ (1 << r)
+            flip = np.where((flip & ((1 << n) - 1)) == 0, best, flip)  # dropping the last one: no change
+            wt[:, r] = obj[rows, flip] - obj[rows, best]
+        y[:, 7] = (best >> n) & 1
+        wt[:, 7] = obj[rows, best ^ (1 << n)] - obj[rows, best]
+        ys.append(y), ws.append(wt)
+    Y, W = np.concatenate(ys), np.concatenate(ws)
+    present = np.zeros_like(W, dtype=bool)
+    k = 0
+    for s in costs:
+        present[k:k + costs[s].shape[0], :nrefs[s]] = True
+        present[k:k + costs[s].shape[0], 7] = True
+        k += costs[s].shape[0]
+    W = np.where(present, np.maximum(W, 0.0), 0.0)
+    W = np.where(present, W / max(W[present].mean(), 1e-12) + floor, 0.0).astype(np.float32)
+    return Y, W

@@ -8,7 +8,9 @@
 2. for every inter frame, every superblock's chosen cost under every mask (data.mask_costs: a
    superblock's decision depends only on its own mask);
 3. the targets: per superblock the mask minimising work + mu * cost increase (data.policy), mu set
-   so that this exact policy loses `--target` (0.4 %) of the summed cost on the training clips;
+   so that this exact policy loses `--target` (0.4 %) of the summed cost on the training clips
+   (`--weighting regret`: each bit weighted by the regret of getting it wrong; on these clips it
+   did not beat uniform weights);
 4. Adam on the weighted cross-entropy of the mask bits, with the library's own kernels;
 5. thresholds: on the validation clips, the fastest setting (device time of the mini-GOP through
    the engine) whose cost rises by at most `--max-loss` (1 %) over the exhaustive search;
@@ -56,6 +58,8 @@ def main():
     ap.add_argument("--target", type=float, default=0.004)
     ap.add_argument("--max-loss", type=float, default=0.01)
     ap.add_argument("--workers", type=int, default=6)
+    ap.add_argument("--weighting", choices=["uniform", "regret"], default="uniform",
+                    help="per-output weights: 1, or the regret of a wrong bit (data.regret_targets)")
     args = ap.parse_args()
     t0 = time.time()
     clips = D.make_clips(TRAIN_SEEDS + VAL_SEEDS + TEST_SEEDS, workers=args.workers)  # before any CUDA use
@@ -80,7 +84,7 @@ def main():
     xs, ys, ws, oracle_work = [], [], [], []
     for feats, costs, nrefs in train_t:
         keeps, work, _ = D.policy(costs, nrefs, mu)
-        y, w = D.policy_labels(keeps, nrefs)
+        y, w = D.regret_targets(costs, nrefs, mu) if args.weighting == "regret" else D.policy_labels(keeps, nrefs)
         xs.append(np.concatenate([feats[s] for s in keeps])), ys.append(y), ws.append(w)
         oracle_work.append(work)
     X, Y, Wt = np.concatenate(xs), np.concatenate(ys), np.concatenate(ws)
@@ -131,7 +135,8 @@ def main():
                  "refs_kept": float(np.mean([r["refs_kept"] for r in v])),
                  "intra_kept": float(np.mean([r["intra_kept"] for r in v]))} for k, v in agg.items()]
 
-    net_settings = [("net", a, b, 0.0) for a in (0.2, 0.3, 0.4, 0.5, 0.6, 0.7) for b in (0.2, 0.3, 0.4, 0.5, 0.6)]
+    net_settings = [("net", a, b, 0.0) for a in (0.3, 0.5, 0.6, 0.7, 0.8, 0.85, 0.9, 0.95)
+                    for b in (0.3, 0.5, 0.7, 0.8, 0.9)]
     val = sweep([nt, nt + 1], net_settings + [("exact",)])
     ok = [r for r in val if r["setting"][0] == "net" and r["loss"] <= args.max_loss]
     best = max(ok, key=lambda r: r["speedup"]) if ok else min((r for r in val if r["setting"][0] == "net"),
@@ -149,7 +154,7 @@ def main():
     os.makedirs(args.out, exist_ok=True)
     np.savez(os.path.join(args.out, "weights.npz"), params=params, ref_threshold=np.float32(tr_),
              intra_threshold=np.float32(ti), band=np.float32(band))
-    report = {"samples": int(X.shape[0]), "steps": args.steps, "batch": args.batch, "loss_curve": losses,
+    report = {"samples": int(X.shape[0]), "steps": args.steps, "weighting": args.weighting, "batch": args.batch, "loss_curve": losses,
               "mu": mu, "target": args.target, "exact_policy_work": float(np.mean(oracle_work)),
               "targets_positive": (Y.sum(0) / np.maximum(Wt.astype(bool).sum(0), 1)).tolist(),
               "validation": val, "chosen": best, "test": test, "exact_policy_curve": curve,
