@@ -10,13 +10,16 @@
 // tiles all sit on the superblock's 4x4 grid), and every candidate MV of a superblock's blocks is
 // the level-0 MV of one of the 10 x 10 cells around it. So one CTA per (superblock, reference):
 //  1. gathers those 100 MVs (clamped into the field) and their distinct set D, and gives every
-//     (block, candidate) slot its MV's index in D, marking repeats of an earlier candidate's MV;
+//     (block, candidate) slot its MV's index in D (the slot's cell is a constant of the block
+//     geometry, tabulated once), and per MV of D the offset of the superblock's prediction in its
+//     phase plane;
 //  2. for chunks of D: one thread per 4x4 tile (its cur samples in registers) computes the tile's
 //     SATD at every MV of the chunk -- a warp reads two contiguous image rows per load -- and the
 //     four tiles of an 8x8 cell, which sit in one warp, sum by shuffles; then the 16x16 sums;
-//  3. every non-repeated slot whose MV is in the chunk takes its SATD from those sums, and a
-//     shared atomicMin of (SATD << 7 | candidate index) keeps each block's least -- the first
-//     strict minimum of the reference's loop over its candidates.
+//  3. every candidate slot whose MV is in the chunk takes its SATD from those sums, and a shared
+//     atomicMin of (SATD << 7 | candidate index) keeps each block's least. That is the reference's
+//     first strict minimum over the candidates in order: a repeated MV (which the reference skips)
+//     has the same SATD as its first occurrence and a larger index, so it never wins.
 // 256 |D| Hadamards per (superblock, reference) instead of up to 68,352 for the blocks one by one.
 // The result per (block, reference) is the winning SATD and MV; the lambda terms are added by the
 // finalize stage, which alone needs the costs.
@@ -30,16 +33,18 @@ constexpr int kChunk = 64;          // distinct MVs per pass at most
 constexpr int kSlots = 4296;        // candidates of the 425 blocks (cells covered + 8 neighbours)
 
 // Where block b's candidate list starts (blocks in index order, mv_candidates() slots each), and
-// for every slot its block and candidate index (b | k << 9).
+// for every slot its block, candidate index and neighbourhood cell (b | k << 9 | cell << 16).
 __constant__ short c_slot_off[kBlocks];
-__device__ unsigned short g_slot[kSlots];
+__device__ unsigned g_slot[kSlots];
 
 struct InterSmem {
   int nb[kNb];  // packed MV of each neighbourhood cell
   int D[kNb];   // distinct MVs, first occurrence order
   int first_idx[kNb];
   unsigned char dmap[kNb];
-  unsigned char list[kSlots];         // per candidate slot: its MV index, 255 where it repeats one
+  int moff[kNb];  // per MV of D: the superblock's prediction, bytes from the reference's level 0
+  unsigned char mfast[kNb];           // per MV of D: its 64 x 64 prediction lies inside the margin
+  unsigned char list[kSlots];         // per candidate slot: its MV index in D
   unsigned key[kBlocks];              // per block: least (SATD << 7 | candidate index) so far
   unsigned short tile[kChunk][256];   // 4x4 SATDs (at most 16 x 4 x 255 = 16,320)
   unsigned short whole8[kChunk][64];  // 8x8 sums (at most 65,280)
@@ -101,7 +106,7 @@ __device__ __forceinline__ int block_satd(const InterSmem& S, int b, int dd) {
 
 // Neighbourhood index (10 x 10, origin one cell above-left of the superblock) of candidate k of
 // the block at superblock-local (bx, by), size bw x bh (candidate_mv_index, inter_common.h:65-78).
-__device__ __forceinline__ int candidate_cell(int bx, int by, int bw, int bh, int k) {
+__host__ __device__ __forceinline__ int candidate_cell(int bx, int by, int bw, int bh, int k) {
   const int lx = bx >> 3, ly = by >> 3;
   const int cw = ((bx + bw - 1) >> 3) - lx + 1, ch = ((by + bh - 1) >> 3) - ly + 1, cells = cw * ch;
   int cx, cy;
@@ -115,10 +120,6 @@ __device__ __forceinline__ int candidate_cell(int bx, int by, int bw, int bh, in
     cy = (n == 1 || n == 4 || n == 5) ? nt : (n == 3 || n == 6 || n == 7) ? nbm : ly;
   }
   return (cy + 1) * 10 + cx + 1;
-}
-
-__device__ __forceinline__ int mv_candidates(int bx, int by, int bw, int bh) {
-  return (((bx + bw - 1) >> 3) - (bx >> 3) + 1) * (((by + bh - 1) >> 3) - (by >> 3) + 1) + 8;
 }
 
 __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __restrict__ jobs, WorkList w, int chunk) {
@@ -167,41 +168,18 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   if (tid < kNb) S.dmap[tid] = (unsigned char)S.first_idx[firstj];
   const int nd = S.nd;
   if (tid == 0 && job.stats) atomicAdd(job.stats + kStatInterMvs, (unsigned long long)nd);
-  __syncthreads();
-  // every candidate slot's MV index (balanced over the threads) ...
-  for (int e = tid; e < kSlots; e += kInterThreads) {
-    const unsigned bp = g_slot[e];
-    const int b = bp & 511, k = bp >> 9;
-    int bx, by, bw, bh;
-    sb_block_geom(b, bx, by, bw, bh);
-    S.list[e] = S.dmap[candidate_cell(bx, by, bw, bh, k)];
+  const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
+  if (tid < nd) {
+    const int m = S.D[tid], mx = mv_x(m), my = mv_y(m), x = ox + (mx >> 2), y = oy + (my >> 2);
+    const long long o = (long long)((my & 3) * 4 + (mx & 3)) * ref.phase + (long long)y * ref.stride + x;
+    S.moff[tid] = (int)o;
+    S.mfast[tid] = inside(ref, x, y, 64, 64) && o == (long long)(int)o;
   }
   __syncthreads();
-  // ... then per block, in candidate order, a repeat of an earlier candidate's MV is marked 255
-  for (int b = tid; b < kBlocks; b += kInterThreads) {
-    int bx, by, bw, bh;
-    sb_block_geom(b, bx, by, bw, bh);
-    unsigned seen0 = 0, seen1 = 0, seen2 = 0, seen3 = 0;
-    unsigned char* L = S.list + c_slot_off[b];
-    const int n = mv_candidates(bx, by, bw, bh);
-    for (int k = 0; k < n; k++) {
-      const int d = L[k];
-      const unsigned bit = 1u << (d & 31);
-      const unsigned seen = d < 32 ? seen0 : d < 64 ? seen1 : d < 96 ? seen2 : seen3;
-      if (seen & bit) {
-        L[k] = 255;
-        continue;
-      }
-      if (d < 32) seen0 |= bit;
-      else if (d < 64) seen1 |= bit;
-      else if (d < 96) seen2 |= bit;
-      else seen3 |= bit;
-    }
-  }
+  for (int e = tid; e < kSlots; e += kInterThreads) S.list[e] = S.dmap[g_slot[e] >> 16];
 
   // this thread's tile: its cur rows, row-transformed, in registers (the grid lies inside the margin)
   const int tx = tid & 15, ty = tid >> 4;
-  const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
   int C[16];
   {
     uint32_t c[4];
@@ -209,6 +187,9 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
     for (int i = 0; i < 4; i++) c[i] = load4(cur.p + (long long)(oy + ty * 4 + i) * cur.stride + ox + tx * 4);
     wh_rows_cur(c, C);
   }
+  // the tile's prediction rows at MV d start at tile_base + moff[d]; words a row apart are ws apart
+  const uintptr_t tile_base = reinterpret_cast<uintptr_t>(ref.p) + (uintptr_t)(ty * 4 * ref.stride + tx * 4);
+  const int ws = ref.stride >> 2;  // strides are multiples of 64
   // chunks of equal size, at most `chunk` MVs each
   const int nchunks = (nd + chunk - 1) / chunk, csize = (nd + nchunks - 1) / nchunks;
   __syncthreads();  // lists complete
@@ -221,16 +202,24 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
       int sat[2];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int m = S.D[c0 + min(dd + h, nc - 1)], mx = mv_x(m), my = mv_y(m);
-        DevPlane ph = ref;
-        ph.p = ref.p + (long long)((my & 3) * 4 + (mx & 3)) * ref.phase;
-        const int x = ox + tx * 4 + (mx >> 2), y = oy + ty * 4 + (my >> 2);
+        const int d = c0 + min(dd + h, nc - 1);
         uint32_t pr[4];
-        if (inside(ph, x, y, 4, 4)) {
-          const uint8_t* p = ph.p + (long long)y * ph.stride + x;
+        if (S.mfast[d]) {  // the usual case, uniform over the CTA: rows from aligned words
+          const uintptr_t a = tile_base + (uintptr_t)(intptr_t)S.moff[d];
+          const uint32_t* wp = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+          const uint32_t sh = (uint32_t)(a & 3) * 8;
+          if (sh == 0) {
 #pragma unroll
-          for (int i = 0; i < 4; i++) pr[i] = load4(p + (long long)i * ph.stride);
+            for (int i = 0; i < 4; i++) pr[i] = __ldg(wp + i * ws);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 4; i++) pr[i] = __funnelshift_r(__ldg(wp + i * ws), __ldg(wp + i * ws + 1), sh);
+          }
         } else {
+          const int m = S.D[d], mx = mv_x(m), my = mv_y(m);
+          DevPlane ph = ref;
+          ph.p = ref.p + (long long)((my & 3) * 4 + (mx & 3)) * ref.phase;
+          const int x = ox + tx * 4 + (mx >> 2), y = oy + ty * 4 + (my >> 2);
 #pragma unroll
           for (int i = 0; i < 4; i++) {
             pr[i] = 0;
@@ -257,12 +246,12 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
       S.sum16[dd][i] = W[c] + W[c + 1] + W[c + 8] + W[c + 9];
     }
     __syncthreads();
-    // 3. every (non-repeated) candidate slot whose MV is in this chunk
+    // 3. every candidate slot whose MV is in this chunk
     for (int e = tid; e < kSlots; e += kInterThreads) {
-      const int d = (int)S.list[e] - c0;  // 255 (a repeat) lies past every chunk
+      const int d = (int)S.list[e] - c0;
       if (d < 0 || d >= nc) continue;
       const unsigned bp = g_slot[e];
-      const int b = bp & 511, k = bp >> 9;
+      const int b = bp & 511, k = (bp >> 9) & 127;
       atomicMin(&S.key[b], ((unsigned)block_satd(S, b, d) << 7) | (unsigned)k);
     }
     __syncthreads();  // the next chunk overwrites the sums
@@ -285,14 +274,15 @@ void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, cudaStream
 
 cudaError_t inter_attributes() {
   short off[kBlocks];
-  unsigned short slot[kSlots];
+  static unsigned slot[kSlots];
   int o = 0;
   for (int b = 0; b < kBlocks; b++) {
     int x, y, w, h;
     sb_block_geom(b, x, y, w, h);
     const int n = ((x + w - 1) / 8 - x / 8 + 1) * ((y + h - 1) / 8 - y / 8 + 1) + 8;
     off[b] = (short)o;
-    for (int k = 0; k < n && o + k < kSlots; k++) slot[o + k] = (unsigned short)(b | (k << 9));
+    for (int k = 0; k < n && o + k < kSlots; k++)
+      slot[o + k] = (unsigned)b | (unsigned)k << 9 | (unsigned)candidate_cell(x, y, w, h, k) << 16;
     o += n;
   }
   if (o != kSlots) return cudaErrorInvalidValue;
