@@ -23,6 +23,8 @@
 // 256 |D| Hadamards per (superblock, reference) instead of up to 68,352 for the blocks one by one.
 // The result per (block, reference) is the winning SATD and MV; the lambda terms are added by the
 // finalize stage, which alone needs the costs.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace celv2cu {
@@ -32,10 +34,13 @@ constexpr int kNb = 100;            // 10 x 10 cells around the superblock
 constexpr int kChunk = 64;          // distinct MVs per pass at most
 constexpr int kSlots = 4296;        // candidates of the 425 blocks (cells covered + 8 neighbours)
 
-// Where block b's candidate list starts (blocks in index order, mv_candidates() slots each), and
-// for every slot its block, candidate index and neighbourhood cell (b | k << 9 | cell << 16).
-__constant__ short c_slot_off[kBlocks];
+// Every (block, candidate) slot as b | k << 9 | cell << 16 (its neighbourhood cell), ordered by
+// block size, block kind, candidate index, block: a warp's slots then take one path through
+// block_satd and name 32 different blocks (no divergence, no colliding shared atomics).
 __device__ unsigned g_slot[kSlots];
+// Block b's candidate k sits in neighbourhood cell g_cand_cell[c_cand_off[b] + k].
+__constant__ short c_cand_off[kBlocks];
+__device__ unsigned char g_cand_cell[kSlots];
 
 struct InterSmem {
   int nb[kNb];  // packed MV of each neighbourhood cell
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   int2* out = job.inter + ((long long)sb * kMaxRefs + r) * kBlocks;
   for (int b = tid; b < kBlocks; b += kInterThreads) {
     const unsigned k = S.key[b];
-    out[b] = make_int2((int)(k >> 7), S.D[S.list[c_slot_off[b] + (k & 127)]]);
+    out[b] = make_int2((int)(k >> 7), S.D[S.dmap[g_cand_cell[c_cand_off[b] + (k & 127)]]]);
   }
   }  // units
 }
@@ -275,18 +280,28 @@ void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, cudaStream
 cudaError_t inter_attributes() {
   short off[kBlocks];
   static unsigned slot[kSlots];
+  static unsigned char cell[kSlots];
+  static unsigned long long order[kSlots];  // sort key << 32 | slot
   int o = 0;
   for (int b = 0; b < kBlocks; b++) {
     int x, y, w, h;
     sb_block_geom(b, x, y, w, h);
     const int n = ((x + w - 1) / 8 - x / 8 + 1) * ((y + h - 1) / 8 - y / 8 + 1) + 8;
+    const int sq = b / 5, size = sq >= 21 ? 3 : sq >= 5 ? 2 : sq >= 1 ? 1 : 0, kind = b - sq * 5;
     off[b] = (short)o;
-    for (int k = 0; k < n && o + k < kSlots; k++)
-      slot[o + k] = (unsigned)b | (unsigned)k << 9 | (unsigned)candidate_cell(x, y, w, h, k) << 16;
+    for (int k = 0; k < n && o + k < kSlots; k++) {
+      const int c = candidate_cell(x, y, w, h, k);
+      cell[o + k] = (unsigned char)c;
+      const unsigned desc = (unsigned)b | (unsigned)k << 9 | (unsigned)c << 16;
+      order[o + k] = (unsigned long long)(size << 19 | kind << 16 | k << 9 | b) << 32 | desc;
+    }
     o += n;
   }
   if (o != kSlots) return cudaErrorInvalidValue;
-  cudaError_t e = cudaMemcpyToSymbol(c_slot_off, off, sizeof off);
+  std::sort(order, order + kSlots);
+  for (int e = 0; e < kSlots; e++) slot[e] = (unsigned)order[e];
+  cudaError_t e = cudaMemcpyToSymbol(c_cand_off, off, sizeof off);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_cand_cell, cell, sizeof cell);
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_slot, slot, sizeof slot);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(k_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InterSmem));
