@@ -13,6 +13,12 @@
 //  3. the 2304 (block, 4x4 tile) items are spread over the threads; each predicts its tile under
 //     the 13 modes from the edge arrays alone (no per-sample rule branches) and takes the
 //     Hadamards; a segmented shuffle reduction sums a block's tiles per mode.
+// The Hadamard of a residual is the cur tile's transform minus the prediction's (linearity), so
+// the cur tile is transformed once per item: its rows by dp4a against the Walsh-Hadamard basis.
+// DC, V and H predictions change only 1, 4 and 4 of the 16 coefficients (a constant tile only the
+// DC; equal rows only the first coefficient of each column transform; constant rows only the
+// first row transform), so those three modes cost a few operations on the cur transform; the ten
+// others pack their prediction rows into bytes and run the dp4a row transform (satd4_rows).
 // The output is raw SATDs; the finalize stage adds lambda * bits (which depend on whether the
 // frame has references, unknown when prepare() runs this ahead of its launch).
 #include "kernels.h"
@@ -43,12 +49,46 @@ __device__ __forceinline__ int edge_offset(int b) {
   return base + idx * per_sq + (kind == 0 ? 0 : (2 * s + 1) + (kind - 1) * (s + s / 2 + 1));
 }
 
-// n / d for 0 <= n < 2^20, from a float estimate corrected to the exact quotient.
-__device__ __forceinline__ int exact_div(int n, int d, float rcp) {
-  int q = __float2int_rz((float)n * rcp);
-  if ((q + 1) * d <= n) q++;
-  if (q * d > n) q--;
-  return q;
+// Rounded blend of p0, p1 with weight sh / 32 (the directional modes' interpolation).
+__device__ __forceinline__ int blend32(int p0, int p1, int sh) { return (p0 * (32 - sh) + p1 * sh + 16) >> 5; }
+
+// Four predicted samples (0..255) as the bytes of one word, sample 0 in the low byte.
+__device__ __forceinline__ uint32_t pack_row(int a, int b, int c, int d) {
+  return (uint32_t)a | (uint32_t)b << 8 | (uint32_t)c << 16 | (uint32_t)d << 24;
+}
+
+// z1 (D45, D67): from the row above, derivative dxa (intra_common.h dir_pred, the z1 branch).
+__device__ __forceinline__ void pred_z1(int dxa, const uint8_t* A, int r0, int c0, int last, uint32_t* pw) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const int pos = (r0 + i + 1) * dxa, b0 = (pos >> 6) + c0, sh = (pos & 63) >> 1;
+    int v[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) v[j] = blend32(A[min(b0 + j, last)], A[min(b0 + j + 1, last)], sh);
+    pw[i] = pack_row(v[0], v[1], v[2], v[3]);
+  }
+}
+
+// z2 (D113, D135, D157): the row above while the projection stays on it, else the left column.
+// (The derivatives stay run-time values: per-mode constants let the compiler spread the three
+// modes' code and spill.)
+__device__ __forceinline__ void pred_z2(int dxa, int dya, const uint8_t* A, const uint8_t* L, int r0, int c0, uint32_t* pw) {
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    int v[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const int ii = r0 + i, jj = c0 + j;
+      const int px = (jj << 6) - (ii + 1) * dxa, bx = px >> 6;
+      if (bx >= -1) {
+        v[j] = blend32(A[bx], A[bx + 1], (px & 63) >> 1);
+      } else {
+        const int py = (ii << 6) - (jj + 1) * dya, by = py >> 6;
+        v[j] = blend32(L[max(by, -1)], L[max(by + 1, -1)], (py & 63) >> 1);
+      }
+    }
+    pw[i] = pack_row(v[0], v[1], v[2], v[3]);
+  }
 }
 
 __global__ void __launch_bounds__(kIntraThreads, 4) k_intra(const FrameJob* __restrict__ jobs, WorkList w) {
@@ -104,131 +144,136 @@ __global__ void __launch_bounds__(kIntraThreads, 4) k_intra(const FrameJob* __re
     const uint8_t* L = S.left + edge_offset(b) + 1;
     const int last = bw + bh - 1;
     const int r0 = ty * 4 - y, c0 = tx * 4 - x;  // the tile's origin inside the block
-    int cur[16];
+    // the cur tile: rows as packed bytes, row-transformed (C), and per basis row k the column
+    // transform's outputs, their absolute sum T, the first outputs Hk0 and their sum V0, and U0
+    // the absolute sum of row k = 0's outputs
+    int C[16];
+    {
+      uint32_t cw[4];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+      for (int i = 0; i < 4; i++) {
+        const uint8_t* q = S.px + (ty * 4 + i + 1) * kRegionStride + tx * 4 + 1;
+        cw[i] = pack_row(q[0], q[1], q[2], q[3]);
+      }
+      wh_rows_cur(cw, C);
+    }
+    const int seg_lead = (tid & ((width < 32 ? width : 32) - 1)) == 0;
+    {
+      // DC, V, H: per basis row k the column transform's outputs; T the sum of all 16 absolute
+      // coefficients (the cur tile's SATD), Hk0 the first outputs and V0 their absolute sum, U0 the
+      // absolute sum of row k = 0's
+      int Hk0[4], T = 0, V0 = 0, U0 = 0;
 #pragma unroll
-      for (int j = 0; j < 4; j++) cur[4 * i + j] = S.px[(ty * 4 + i + 1) * kRegionStride + tx * 4 + j + 1];
+      for (int k = 0; k < 4; k++) {
+        const int s01 = C[4 * k] + C[4 * k + 1], d01 = C[4 * k] - C[4 * k + 1];
+        const int s23 = C[4 * k + 2] + C[4 * k + 3], d23 = C[4 * k + 2] - C[4 * k + 3];
+        const int a = abs(s01 + s23) + abs(s01 - s23) + abs(d01 + d23) + abs(d01 - d23);
+        T += a, Hk0[k] = s01 + s23, V0 += abs(s01 + s23);
+        if (k == 0) U0 = a;
+      }
+      // DC: only coefficient (0, 0) moves, by 16 v
+      const int dc = T - abs(Hk0[0]) + abs(Hk0[0] - 16 * S.dc[b]);
+      // V: every row is the above row a; the first output of each column transform moves by 4 a_k
+      const uint32_t a = pack_row(A[c0], A[c0 + 1], A[c0 + 2], A[c0 + 3]);
+      int v = T - V0;
+#pragma unroll
+      for (int k = 0; k < 4; k++) v += abs(Hk0[k] - 4 * dp4a_us(a, wh_row(k), 0));
+      // H: row i is the constant l_i; row transform k = 0 moves by 4 l_i
+      const int r0v = C[0] - 4 * L[r0], r1v = C[1] - 4 * L[r0 + 1];
+      const int r2v = C[2] - 4 * L[r0 + 2], r3v = C[3] - 4 * L[r0 + 3];
+      const int s01 = r0v + r1v, d01 = r0v - r1v, s23 = r2v + r3v, d23 = r2v - r3v;
+      const int h = T - U0 + abs(s01 + s23) + abs(s01 - s23) + abs(d01 + d23) + abs(d01 - d23);
+      const int s0 = segment_sum(dc, width), s1 = segment_sum(v, width), s2 = segment_sum(h, width);
+      if (seg_lead) atomicAdd(&S.acc[b][0], s0), atomicAdd(&S.acc[b][1], s1), atomicAdd(&S.acc[b][2], s2);
+    }
     const int lgw = 31 - __clz(bw), lgh = 31 - __clz(bh);
     const int den = bw + bh + 2;
-    const float rcp = 1.0f / (float)den;
+    // n / den for n < 2^15 as a multiply-high by ceil(2^32 / den): exact while n * (den * ceil(2^32 /
+    // den) - 2^32) < 2^32 (division by invariant integers using multiplication, Granlund and
+    // Montgomery 1994); here n < 256 den and den <= 66
+    const unsigned magic = 0xffffffffu / (unsigned)den + 1u;
 #pragma unroll 1
-    for (int m = 0; m < kModes; m++) {
-      int d[16];
+    for (int m = 3; m < kModes; m++) {  // the ten modes with their own prediction rows
+      uint32_t pw[4];
       switch (m) {
-        case 0: {
-          const int v = S.dc[b];
-#pragma unroll
-          for (int k = 0; k < 16; k++) d[k] = cur[k] - v;
-          break;
-        }
-        case 1:
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) d[4 * i + j] = cur[4 * i + j] - A[c0 + j];
-          break;
-        case 2:
-#pragma unroll
-          for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) d[4 * i + j] = cur[4 * i + j] - L[r0 + i];
-          break;
         case 3: {  // Smooth: bilinear blend of above, left, top-right and bottom-left
           const int tr = A[bw - 1], bl = L[bh - 1];
 #pragma unroll
-          for (int i = 0; i < 4; i++)
+          for (int i = 0; i < 4; i++) {
+            int v[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
               const int ii = r0 + i, jj = c0 + j;
               const int num = (bh - ii) * A[jj] + (ii + 1) * bl + (bw - jj) * L[ii] + (jj + 1) * tr;
-              d[4 * i + j] = cur[4 * i + j] - exact_div(num + den / 2, den, rcp);
+              v[j] = (int)__umulhi((unsigned)(num + den / 2), magic);
             }
+            pw[i] = pack_row(v[0], v[1], v[2], v[3]);
+          }
           break;
         }
         case 4: {  // SmoothV (h is a power of two, the numerator non-negative)
           const int bl = L[bh - 1];
 #pragma unroll
-          for (int i = 0; i < 4; i++)
+          for (int i = 0; i < 4; i++) {
+            const int ii = r0 + i;
+            int v[4];
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-              const int ii = r0 + i;
-              d[4 * i + j] = cur[4 * i + j] - (((bh - 1 - ii) * A[c0 + j] + (ii + 1) * bl + bh / 2) >> lgh);
-            }
+            for (int j = 0; j < 4; j++) v[j] = ((bh - 1 - ii) * A[c0 + j] + (ii + 1) * bl + bh / 2) >> lgh;
+            pw[i] = pack_row(v[0], v[1], v[2], v[3]);
+          }
           break;
         }
         case 5: {  // SmoothH
           const int tr = A[bw - 1];
 #pragma unroll
-          for (int i = 0; i < 4; i++)
+          for (int i = 0; i < 4; i++) {
+            int v[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
               const int jj = c0 + j;
-              d[4 * i + j] = cur[4 * i + j] - (((bw - 1 - jj) * L[r0 + i] + (jj + 1) * tr + bw / 2) >> lgw);
+              v[j] = ((bw - 1 - jj) * L[r0 + i] + (jj + 1) * tr + bw / 2) >> lgw;
             }
+            pw[i] = pack_row(v[0], v[1], v[2], v[3]);
+          }
           break;
         }
         case 6: {  // Paeth
           const int tl = A[-1];
 #pragma unroll
-          for (int i = 0; i < 4; i++)
+          for (int i = 0; i < 4; i++) {
+            int v[4];
 #pragma unroll
             for (int j = 0; j < 4; j++) {
               const int a = A[c0 + j], l = L[r0 + i], bse = a + l - tl;
               const int pa = abs(bse - a), pl = abs(bse - l), ptl = abs(bse - tl);
-              d[4 * i + j] = cur[4 * i + j] - (pl <= pa && pl <= ptl ? l : pa <= ptl ? a : tl);
+              v[j] = pl <= pa && pl <= ptl ? l : pa <= ptl ? a : tl;
             }
-          break;
-        }
-        case 7:
-        case 8: {  // z1: D45 (derivative 64), D67 (27), from the row above
-          const int dxa = m == 7 ? 64 : 27;
-#pragma unroll
-          for (int i = 0; i < 4; i++) {
-            const int pos = (r0 + i + 1) * dxa, b0 = (pos >> 6) + c0, sh = (pos & 63) >> 1;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-              const int p0 = A[min(b0 + j, last)], p1 = A[min(b0 + j + 1, last)];
-              d[4 * i + j] = cur[4 * i + j] - ((p0 * (32 - sh) + p1 * sh + 16) >> 5);
-            }
+            pw[i] = pack_row(v[0], v[1], v[2], v[3]);
           }
           break;
         }
-        case 12: {  // z3: D203 (derivative 27), from the column left
+        case 7:
+        case 8: pred_z1(m == 7 ? 64 : 27, A, r0, c0, last, pw); break;  // D45, D67
+        case 9:
+        case 10:
+        case 11:  // D113, D135, D157
+          pred_z2(m == 9 ? 27 : m == 10 ? 64 : 151, m == 9 ? 151 : m == 10 ? 64 : 27, A, L, r0, c0, pw);
+          break;
+        default: {  // z3: D203 (derivative 27), from the column left
+          int v[16];
 #pragma unroll
           for (int j = 0; j < 4; j++) {
             const int pos = (c0 + j + 1) * 27, b0 = (pos >> 6) + r0, sh = (pos & 63) >> 1;
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-              const int p0 = L[min(b0 + i, last)], p1 = L[min(b0 + i + 1, last)];
-              d[4 * i + j] = cur[4 * i + j] - ((p0 * (32 - sh) + p1 * sh + 16) >> 5);
-            }
+            for (int i = 0; i < 4; i++) v[4 * i + j] = blend32(L[min(b0 + i, last)], L[min(b0 + i + 1, last)], sh);
           }
-          break;
-        }
-        default: {  // z2: D113, D135, D157 -- the row above while the projection stays on it
-          const int dxa = m == 9 ? 27 : m == 10 ? 64 : 151, dya = m == 9 ? 151 : m == 10 ? 64 : 27;
 #pragma unroll
-          for (int i = 0; i < 4; i++)
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-              const int ii = r0 + i, jj = c0 + j;
-              const int px = (jj << 6) - (ii + 1) * dxa, bx = px >> 6;
-              int p;
-              if (bx >= -1) {
-                const int sh = (px & 63) >> 1;
-                p = (A[bx] * (32 - sh) + A[bx + 1] * sh + 16) >> 5;
-              } else {
-                const int py = (ii << 6) - (jj + 1) * dya, by = py >> 6, sh = (py & 63) >> 1;
-                p = (L[max(by, -1)] * (32 - sh) + L[max(by + 1, -1)] * sh + 16) >> 5;
-              }
-              d[4 * i + j] = cur[4 * i + j] - p;
-            }
+          for (int i = 0; i < 4; i++) pw[i] = pack_row(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
           break;
         }
       }
-      const int s = segment_sum(hadamard4x4(d), width);
-      if ((tid & ((width < 32 ? width : 32) - 1)) == 0) atomicAdd(&S.acc[b][m], s);
+      const int s = segment_sum(satd4_rows(C, pw), width);
+      if (seg_lead) atomicAdd(&S.acc[b][m], s);
     }
   }
   __syncthreads();
