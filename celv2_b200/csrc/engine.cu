@@ -110,6 +110,8 @@ void init_device(int dev) {
   CK(inter_attributes());
   CK(intra_attributes());
   CK(finalize_attributes());
+  // the constant tables' copies (from pageable memory) land before any kernel on another stream
+  CK(cudaDeviceSynchronize());
   g_ready[dev] = 1;
 }
 
@@ -1369,7 +1371,9 @@ int celv2_set_pruner(celv2_engine* e, const float* params, float ref_threshold, 
       CK(cudaMalloc(&e->pruner_params, CELV2_PRUNER_PARAMS * sizeof(float)));
       CK(cudaMalloc(&e->nn_wb, infer_weight_elems() * 2));
     }
-    CK(cudaMemcpy(e->pruner_params, params, CELV2_PRUNER_PARAMS * sizeof(float), cudaMemcpyHostToDevice));
+    // on the engine's stream, ahead of the kernel that reads them (a synchronous copy from pageable
+    // memory may return before its DMA lands, and the engine's streams do not wait for it)
+    CK(cudaMemcpyAsync(e->pruner_params, params, CELV2_PRUNER_PARAMS * sizeof(float), cudaMemcpyHostToDevice, e->st));
     infer_weights(e->pruner_params, e->nn_wb, e->st);
     CK(cudaStreamSynchronize(e->st));
     e->pruner_tr = ref_threshold, e->pruner_ti = intra_threshold, e->pruner_band = band;

@@ -253,7 +253,9 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
 constexpr int kRefineCells = 7, kRefineThreads = 256;  // 7 x 36 = 252 items
 
 __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
-  __shared__ int cc[kRefineCells][4][16];
+  // per (cell, tile) its 16 row coefficients, 17 words apart: the tiles and cells one warp reads
+  // at once fall in different banks
+  __shared__ int cc[kRefineCells * 4][17];
   __shared__ int sat[kRefineCells][9];
   __shared__ int mvx[kRefineCells], mvy[kRefineCells], need[kRefineCells];
   __shared__ int unit_slot;
@@ -274,7 +276,7 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob*
     const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
     const uint32_t cw = row4(cur, bx * 8 + 4 * (t & 1), by * 8 + 4 * (t >> 1) + i);
 #pragma unroll
-    for (int k = 0; k < 4; k++) cc[c][t][4 * k + i] = dp4a_us(cw, wh_row(k), 0);
+    for (int k = 0; k < 4; k++) cc[c * 4 + t][4 * k + i] = dp4a_us(cw, wh_row(k), 0);
   }
   if (tid < ncells) {
     const int m = field[cell0 + tid];
@@ -303,7 +305,7 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob*
 #pragma unroll
       for (int i = 0; i < 4; i++) pr[i] = row4(ph, x, y + i);
     }
-    int v = satd4_rows(cc[c][tile], pr);  // the cur coefficients read from shared memory as used
+    int v = satd4_rows(cc[c * 4 + tile], pr);  // the cur coefficients read from shared memory as used
     v += __shfl_xor_sync(0xffffffffu, v, 1);
     v += __shfl_xor_sync(0xffffffffu, v, 2);
     if (valid && tile == 0) sat[c][t] = v;
