@@ -370,8 +370,9 @@ def run_e2e(eng, clip, plan, steps, dist, local, world):
       value     -- the mini-GOP through CudaEngine.decide_group (celv2_upload_pinned,
                    celv2_set_output, celv2_launch_group) from page-locked host planes (a frame pool,
                    filled once before timing): groups issued back to back, the planes copied by DMA
-                   and the records straight into the DecisionMaps while the next group runs; the step
-                   ends when all are in host memory.
+                   and the records straight into the DecisionMaps while the next group runs; the ten
+                   leaves as two batches of five, so the first half's records copy while the second
+                   half is decided; the step ends when all are in host memory.
       per_group -- the same, waiting for each group's records before the next group is issued.
       pageable  -- `value` from ordinary (pageable) numpy planes: celv2_upload copies each into
                    a staging buffer on the host first.
@@ -384,6 +385,9 @@ def run_e2e(eng, clip, plan, steps, dist, local, world):
 
     nsb = eng.sb_cols * eng.sb_rows
     plane = clip[0].hy.nbytes
+    leaves = plan[-1]
+    half = (len(leaves) + 1) // 2
+    plan = plan[:-1] + [leaves[:half], leaves[half:]]  # the leaves' records copy while the rest run
     pool = []  # the page-locked frame pool (an encoder keeps its source frames in one)
     for f in clip:
         a = E.host_array(f.hy.shape, np.uint16)
@@ -444,7 +448,7 @@ def run_e2e(eng, clip, plan, steps, dist, local, world):
             "d2h_bytes_per_step": NFRAMES * nsb * RECORD_BYTES, "steps": steps,
             "api": "CudaEngine.decide_group per coding group (celv2_upload_pinned, celv2_set_output, "
                    "celv2_launch_group) from a page-locked frame pool; records straight into host DecisionMaps, "
-                   "copies overlapping the next group",
+                   "copies overlapping the next group; the ten leaves as two batches of five",
             "per_group": {"value": per_group, "note": "each group's records in host memory before the next group"},
             "pageable": {"value": pageable, "note": "the same from pageable numpy planes (celv2_upload)"},
             "per_frame": {"value": per_frame, "h2d_bytes_per_step": (NFRAMES + len(ref_frames)) * plane,
