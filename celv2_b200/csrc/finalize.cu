@@ -37,7 +37,7 @@ struct FinSmem {
   int ntree, nblocks;
 };
 
-__global__ void __launch_bounds__(kFinThreads, 3) k_finalize(const FrameJob* __restrict__ jobs, WorkList w) {
+__global__ void __launch_bounds__(kFinThreads, 4) k_finalize(const FrameJob* __restrict__ jobs, WorkList w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   FinSmem& S = *reinterpret_cast<FinSmem*>(smem_raw);
   __shared__ int unit_slot;
