@@ -2,7 +2,7 @@
 // CpuEngine and decide_*_ref rules: the engine tests of the reference (tests/test_gpu_intra.cpp,
 // tests/test_gpu_me.cpp) with CudaEngine in the place of VulkanEngine. Built by oracle/Makefile
 // (target adapter-test) from the reference's sources and test headers where they lie; run by
-// tests/test_gpu_adapter.py on a GPU box. Exit status 0 when every case passes.
+// tests/test_gpu_adapter.py on a machine with a B200. Exit status 0 when every case passes.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
