@@ -868,6 +868,9 @@ struct celv2_engine {
     const std::array<celv2_sb_out*, kMaxJobs> dests = take_outputs();
     const std::array<std::vector<uint8_t>, kMaxJobs> keeps = take_keeps();
     if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per group");
+    if (!to_host)
+      for (int j = 0; j < njobs; j++)
+        if (dests[j]) invalid("group: set_output names host memory, but to_host 0 leaves the records on the device");
     if (njobs > group_cap) reserve_group(std::max(njobs, 8));
     std::vector<FrameJob> jobs(njobs);
     std::vector<Slot*> reads;
@@ -875,6 +878,7 @@ struct celv2_engine {
       Slot* cur = find(src_keys[j]);
       if (!cur) invalid("group: no stored frame with the source key");
       if (nrefs[j] < 0 || nrefs[j] > kMaxRefs) invalid("group: too many references");
+      if (nrefs[j] > 0 && !ref_keys) invalid("group: null reference keys");
       if (nrefs[j] > 0 && (g.pw < 16 || g.ph < 16)) invalid("group: inter frames need at least 9x9 pixels");
       Slot* refs[kMaxRefs];
       for (int r = 0; r < nrefs[j]; r++) {
@@ -913,7 +917,7 @@ struct celv2_engine {
       CK(cudaEventRecord(copied[par], copy_st));
       copy_pending[par] = true;
     } else {
-      for (int j = 0; j < njobs; j++) group_out[j] = group_host + (size_t)j * g.nsb;
+      for (int j = 0; j < njobs; j++) group_out[j] = nullptr;  // records left on the device
     }
     group_jobs = njobs;
     ++launches;
@@ -1000,6 +1004,26 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     if (!engines[j]) invalid("null engine");
     if (engines[j]->device != lead->device) invalid("a batch runs on one GPU");
   }
+  if (!to_host)
+    for (const auto& d : dests)
+      for (celv2_sb_out* p : d)
+        if (p) invalid("batch: set_output names host memory, but to_host 0 leaves the records on the device");
+  // Every key and reference is checked before any state changes (record buffer parities, waits,
+  // phase planes), so a rejected batch leaves every engine as it was.
+  std::vector<Slot*> cur_of(njobs);
+  std::vector<std::array<Slot*, kMaxRefs>> refs_of(njobs);
+  for (int j = 0; j < njobs; j++) {
+    celv2_engine* e = engines[j];
+    cur_of[j] = e->find(src_keys[j]);
+    if (!cur_of[j]) invalid("batch: no stored frame with the source key");
+    if (nrefs[j] < 0 || nrefs[j] > kMaxRefs) invalid("batch: too many references");
+    if (nrefs[j] > 0 && !ref_keys) invalid("batch: null reference keys");
+    if (nrefs[j] > 0 && (e->g.pw < 16 || e->g.ph < 16)) invalid("batch: inter frames need at least 9x9 pixels");
+    for (int r = 0; r < nrefs[j]; r++) {
+      refs_of[j][r] = e->find(ref_keys[j][r]);
+      if (!refs_of[j][r]) invalid("batch: no stored frame with a reference key");
+    }
+  }
   for (celv2_engine* e : uniq) {
     int count = 0;
     for (int j = 0; j < njobs; j++) count += engines[j] == e;
@@ -1031,15 +1055,8 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     celv2_engine* e = engines[j];
     const int ei = (int)(std::find(uniq.begin(), uniq.end(), e) - uniq.begin());
     const int slot = next[ei]++;
-    Slot* cur = e->find(src_keys[j]);
-    if (!cur) invalid("batch: no stored frame with the source key");
-    if (nrefs[j] < 0 || nrefs[j] > kMaxRefs) invalid("batch: too many references");
-    if (nrefs[j] > 0 && (e->g.pw < 16 || e->g.ph < 16)) invalid("batch: inter frames need at least 9x9 pixels");
-    Slot* refs[kMaxRefs];
-    for (int r = 0; r < nrefs[j]; r++) {
-      refs[r] = e->find(ref_keys[j][r]);
-      if (!refs[r]) invalid("batch: no stored frame with a reference key");
-    }
+    Slot* cur = cur_of[j];
+    Slot* const* refs = refs_of[j].data();
     e->wait_ready(*cur, lead->st);
     reads[ei].push_back(cur);
     for (int r = 0; r < nrefs[j]; r++) {
@@ -1068,10 +1085,13 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     CK(cudaStreamWaitEvent(lead->copy_st, lead->stages_done, 0));
   }
   for (const Entry& en : entries) {
-    celv2_sb_out* d = en.dest && to_host ? en.dest : en.e->group_host + (size_t)en.slot * en.e->g.nsb;
+    if (!to_host) {
+      en.e->group_out[en.slot] = nullptr;  // records left on the device
+      continue;
+    }
+    celv2_sb_out* d = en.dest ? en.dest : en.e->group_host + (size_t)en.slot * en.e->g.nsb;
     en.e->group_out[en.slot] = d;
-    if (to_host)
-      CK(cudaMemcpyAsync(d, en.job.out, en.e->g.nsb * sizeof(celv2_sb_out), cudaMemcpyDeviceToHost, lead->copy_st));
+    CK(cudaMemcpyAsync(d, en.job.out, en.e->g.nsb * sizeof(celv2_sb_out), cudaMemcpyDeviceToHost, lead->copy_st));
   }
   if (to_host)
     for (size_t i = 0; i < uniq.size(); i++) {
@@ -1242,6 +1262,8 @@ int celv2_group_records(celv2_engine* e, int job, const celv2_sb_out** records) 
   return guarded([&] {
     if (!e || !records) invalid("null argument");
     if (job < 0 || job >= e->group_jobs) invalid("no such job in the last group");
+    if (!e->group_out[job])
+      throw Error(CELV2_ESTATE, "group_records: the last group left its records on the device (to_host 0)");
     CK(cudaSetDevice(e->device));
     e->wait_idle();
     *records = e->group_out[job];

@@ -21,7 +21,9 @@
 //  - every call shares the array and it keeps the last call's contents. Each call rewrites all of
 //    the scratch it reads (every SATD entry of every superblock it decides, and the descriptor),
 //    so nothing has to start at zero; but calls whose GPU work overlaps (on different streams, or
-//    from threads that do not order their calls) race on the array.
+//    from threads that do not order their calls) race on the array;
+//  - the job descriptor reaches the array as a kernel parameter (k_put_job), so no host memory is
+//    read after the call returns.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -43,6 +45,7 @@ using namespace celv2cu;
 namespace {
 
 constexpr int kMaxSb = CELV2_NOALLOC_MAX_SUPERBLOCKS;
+constexpr int kMaxSide = 1 << 16;  // width, height and pitch bound (samples)
 // The descriptor first (rounded up to 256 bytes), then the intra SATDs of kMaxSb superblocks.
 constexpr size_t kJobInts = (sizeof(FrameJob) + 255) / 256 * 64;
 constexpr size_t kScratchInts = kJobInts + (size_t)kMaxSb * kBlocks * kModes;
@@ -53,6 +56,12 @@ std::mutex g_mu;
 std::vector<int*> g_scratch_addr;  // per device: the array's device address, once looked up
 
 // The device address of the array on the current device `dev` (set up on the first call).
+// Writes the job descriptor into the scratch array. The descriptor travels as a kernel parameter,
+// which the launch copies, so nothing on the host is read once the call has returned.
+__global__ void k_put_job(FrameJob job, FrameJob* dst) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = job;
+}
+
 int* scratch_on(int dev) {
   std::lock_guard<std::mutex> lk(g_mu);
   if ((int)g_scratch_addr.size() <= dev) g_scratch_addr.resize(dev + 1, nullptr);
@@ -77,6 +86,13 @@ extern "C" int celv2_decide_key_noalloc(const uint8_t* luma, int width, int heig
   }
   if (width <= 0 || height <= 0) {
     set_last_error("decide_key_noalloc: frame size must be positive");
+    return CELV2_EINVAL;
+  }
+  // bounded before any arithmetic on the sizes (no int overflow); the superblock limit below is
+  // far tighter for any real frame
+  if (width > kMaxSide || height > kMaxSide || pitch > kMaxSide) {
+    set_last_error("decide_key_noalloc: width, height and pitch must be at most " + std::to_string(kMaxSide) +
+                   " (and the frame within " + std::to_string(kMaxSb) + " superblocks)");
     return CELV2_EINVAL;
   }
   const int pw = (width + 7) & ~7, ph = (height + 7) & ~7;
@@ -117,8 +133,8 @@ extern "C" int celv2_decide_key_noalloc(const uint8_t* luma, int width, int heig
   job.stats = nullptr;
   FrameJob* djob = reinterpret_cast<FrameJob*>(scratch);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // a copy of a host stack object: consumed before the call returns
-  e = cudaMemcpyAsync(djob, &job, sizeof job, cudaMemcpyHostToDevice, st);
+  k_put_job<<<1, 32, 0, st>>>(job, djob);
+  e = cudaGetLastError();
   if (e == cudaSuccess) {
     WorkList w{};
     w.njobs = 1;

@@ -178,3 +178,53 @@ def test_pinned_uploads_match_oracle(oracle):
         for g, dms in zip(groups, out):
             for (s, refs), dm in zip(g, dms):
                 check(oracle, w, h, clip, s, refs, 120, dm.records, f"frame {s}")
+
+
+def test_records_left_on_the_device_are_not_returned(oracle):
+    """A group launched with to_host 0 leaves its records on the device: group_records refuses it
+    (rather than returning an older group's records), and set_output is refused for such a launch."""
+    w, h = 416, 240
+    clip = synth.small_clip(seed=27, frames=4)
+    with E.CudaEngine(w, h) as e:
+        for i, f in enumerate(clip):
+            e.upload(f.hy, i)
+        e.launch_group([3], [[2, 1]], 120, to_host=True)
+        check(oracle, w, h, clip, 3, [2, 1], 120, e.group_records(0), "to_host group")
+        e.launch_group([2], [[1]], 120, to_host=False)
+        with pytest.raises(RuntimeError, match="on the device"):
+            e.group_records(0)
+        out = E.host_array((e.sb_cols * e.sb_rows * SB_OUT_DTYPE.itemsize,), np.uint8)
+        e.set_output(0, out.ctypes.data)
+        with pytest.raises(RuntimeError, match="to_host 0"):
+            e.launch_group([2], [[1]], 120, to_host=False)
+        e.launch_group([2], [[1]], 120, to_host=True)
+        check(oracle, w, h, clip, 2, [1], 120, e.group_records(0), "after the refused launch")
+
+
+def test_rejected_multi_batch_leaves_the_engines_as_they_were(oracle):
+    """A batch with a missing reference key is rejected before it changes any engine's state; the
+    next two batches, both in flight before either is read, still give the oracle's records."""
+    sizes = [(416, 240), (202, 122)]
+    clips = [synth.sinusoid_clip(w, h, 3, 60 + k, noise_sigma=3.0) for k, (w, h) in enumerate(sizes)]
+    engines = [E.CudaEngine(w, h) for w, h in sizes]
+    try:
+        for e, clip in zip(engines, clips):
+            for i, f in enumerate(clip):
+                e.upload(f.hy, i)
+        with pytest.raises(RuntimeError, match="reference key"):
+            E.launch_multi([(engines[0], 2, [1, 0]), (engines[1], 2, [99])], 130, to_host=True)
+        batches = [[(engines[0], 2, [1, 0]), (engines[1], 2, [1])], [(engines[1], 1, [0]), (engines[0], 1, [0])]]
+        maps = []
+        for jobs in batches:
+            dms = [DecisionMap() for _ in jobs]
+            E.launch_multi(jobs, 130, dms=dms)
+            maps.append(dms)
+        for e in engines:
+            e.finish()
+        for jobs, dms in zip(batches, maps):
+            for (e, src, refs), dm in zip(jobs, dms):
+                i = engines.index(e)
+                check(oracle, *sizes[i], clips[i], src, refs, 130, dm.records, f"{sizes[i]} frame {src}")
+    finally:
+        for e in engines:
+            e.close()
