@@ -16,6 +16,8 @@ rounded to 8 bits (``round_to_8bit``), exactly as the reference's y4m reader han
 """
 from __future__ import annotations
 
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 
 import numpy as np
@@ -28,6 +30,7 @@ __all__ = [
     "animation_clip",
     "small_clip",
     "hd_clip",
+    "anime_clip",
     "write_y4m",
 ]
 
@@ -122,14 +125,9 @@ def sinusoid_clip(
         trans = rng.uniform(-affine_motion, affine_motion, (nreg, 2))
         rot = rng.uniform(-0.01, 0.01, nreg)  # radians per frame
         zoom = rng.uniform(-0.01, 0.01, nreg)  # relative scale per frame
-    yy, xx = np.mgrid[0:height, 0:width].astype(np.float64)
-    gpos = np.zeros(2)
-    rpos = np.zeros((rects, 2))
-    out = []
-    for t in range(frames):
-        if t > 0:
-            gpos += np.round(rng.uniform(-global_motion, global_motion, 2) * 4) / 4
-            rpos += np.round(rng.uniform(-rect_motion, rect_motion, (rects, 2)) * 4) / 4
+    def render(r0: int, r1: int, t: int, gpos: np.ndarray, rpos: np.ndarray) -> np.ndarray:
+        """Rows r0 .. r1 of frame t before the noise (every sample depends on its position only)."""
+        yy, xx = np.mgrid[r0:r1, 0:width].astype(np.float64)
         if affine_regions:
             # each pixel's region; its content comes from the region's affine map at frame t
             reg = (np.minimum(yy * gy // height, gy - 1) * gx + np.minimum(xx * gx // width, gx - 1)).astype(int)
@@ -142,7 +140,7 @@ def sinusoid_clip(
             sy = (np.sin(a) * dx + np.cos(a) * dy) * s + cy - trans[reg, 1] * t
         else:
             sx, sy = xx - gpos[0], yy - gpos[1]
-        v = np.full((height, width), 512.0)
+        v = np.full((r1 - r0, width), 512.0)
         for k in range(sinusoids):
             v += amps[k] * np.sin(kx[k] * sx + ky[k] * sy + phases[k])
         for k in range(rects):
@@ -150,8 +148,24 @@ def sinusoid_clip(
             y0 = ry0[k] + rpos[k, 1]
             m = (sx >= x0) & (sx < x0 + rw[k]) & (sy >= y0) & (sy < y0 + rh[k])
             v[m] = rlevel[k]
-        v += rng.normal(0.0, noise_sigma, v.shape)
-        out.append(_make_frame(np.clip(v, 64, 960), width, height, with_chroma))
+        return v
+
+    # row bands on threads (numpy releases the GIL inside the array arithmetic); the noise is drawn
+    # for the whole frame in order, so the clip does not depend on the band count
+    bands = max(1, min(16, os.cpu_count() or 1, height // 64))
+    edges = [height * i // bands for i in range(bands + 1)]
+    gpos = np.zeros(2)
+    rpos = np.zeros((rects, 2))
+    out = []
+    with ThreadPoolExecutor(bands) as pool:
+        for t in range(frames):
+            if t > 0:
+                gpos += np.round(rng.uniform(-global_motion, global_motion, 2) * 4) / 4
+                rpos += np.round(rng.uniform(-rect_motion, rect_motion, (rects, 2)) * 4) / 4
+            parts = pool.map(lambda i: render(edges[i], edges[i + 1], t, gpos.copy(), rpos.copy()), range(bands))
+            v = np.concatenate(list(parts), axis=0)
+            v += rng.normal(0.0, noise_sigma, v.shape)
+            out.append(_make_frame(np.clip(v, 64, 960), width, height, with_chroma))
     return out
 
 
@@ -161,7 +175,7 @@ def animation_clip(
     frames: int,
     seed: int,
     *,
-    colours: int = 16,
+    colours: int | tuple[int, int] = (8, 24),
     pieces: tuple[int, int] = (4, 3),
     motion: float = 48.0,
     noisy_fraction: float = 0.005,
@@ -169,11 +183,17 @@ def animation_clip(
     scene_cut: int | None = None,
     with_chroma: bool = False,
 ) -> list[Frame]:
-    """Flat colour regions with hard edges, piecewise-translational motion, optional scene cut."""
+    """Flat colour regions with 1-px hard edges (40 rectangles and ellipses drawn over a background,
+    each of one palette colour), sparse noisy pixels, piecewise-translational motion (a grid of
+    `pieces` regions, each moving by its own whole-pel velocity, up to `motion` px per frame) and an
+    optional scene cut (a new palette, new shapes and new velocities from frame `scene_cut` on).
+    `colours`: the palette size, or a (low, high) range it is drawn from per scene."""
     rng = np.random.default_rng(seed)
+    px, py = pieces
 
     def scene(r: np.random.Generator):
-        pal = r.uniform(64.0, 960.0, colours)
+        n = colours if isinstance(colours, int) else int(r.integers(colours[0], colours[1] + 1))
+        pal = r.uniform(64.0, 960.0, n)
         nshapes = 40
         shapes = np.stack(
             [
@@ -181,18 +201,18 @@ def animation_clip(
                 r.uniform(-height * 0.2, height * 1.2, nshapes),
                 r.uniform(width * 0.03, width * 0.3, nshapes),
                 r.uniform(height * 0.03, height * 0.3, nshapes),
-                r.integers(0, colours, nshapes).astype(float),
+                r.integers(0, n, nshapes).astype(float),
                 r.integers(0, 2, nshapes).astype(float),
             ],
             axis=1,
         )
-        vel = r.uniform(-motion, motion, (pieces[0] * pieces[1], 2)).round()
+        vel = r.uniform(-motion, motion, (px * py, 2)).round()
         return pal, shapes, vel
 
+    # piece k covers columns xs[k % px] .. xs[k % px + 1] and rows ys[k // px] .. ys[k // px + 1]
+    xs = [-(-i * width // px) for i in range(px + 1)]
+    ys = [-(-j * height // py) for j in range(py + 1)]
     pal, shapes, vel = scene(rng)
-    yy, xx = np.mgrid[0:height, 0:width].astype(np.float64)
-    px, py = pieces
-    piece = (np.minimum(yy * py // height, py - 1) * px + np.minimum(xx * px // width, px - 1)).astype(int)
     out = []
     t0 = 0
     for t in range(frames):
@@ -200,15 +220,25 @@ def animation_clip(
             pal, shapes, vel = scene(rng)
             t0 = t
         dt = t - t0
-        sx = xx - vel[piece, 0] * dt
-        sy = yy - vel[piece, 1] * dt
         v = np.full((height, width), pal[0])
-        for x0, y0, w, h, c, ell in shapes:
-            if ell:
-                m = ((sx - x0) / w) ** 2 + ((sy - y0) / h) ** 2 < 1.0
-            else:
-                m = (sx >= x0) & (sx < x0 + w) & (sy >= y0) & (sy < y0 + h)
-            v[m] = pal[int(c)]
+        for k in range(px * py):
+            ax0, ax1, ay0, ay1 = xs[k % px], xs[k % px + 1], ys[k // px], ys[k // px + 1]
+            ox, oy = vel[k, 0] * dt, vel[k, 1] * dt  # the piece shows the scene at (x - ox, y - oy)
+            for x0, y0, w, h, c, ell in shapes:
+                # the shape's extent in frame coordinates, one pixel of slack, clipped to the piece
+                lo_x, hi_x = (x0 - w, x0 + w) if ell else (x0, x0 + w)
+                lo_y, hi_y = (y0 - h, y0 + h) if ell else (y0, y0 + h)
+                bx0, bx1 = max(ax0, int(np.floor(lo_x + ox)) - 1), min(ax1, int(np.ceil(hi_x + ox)) + 1)
+                by0, by1 = max(ay0, int(np.floor(lo_y + oy)) - 1), min(ay1, int(np.ceil(hi_y + oy)) + 1)
+                if bx0 >= bx1 or by0 >= by1:
+                    continue
+                sx = np.arange(bx0, bx1, dtype=np.float64)[None, :] - ox
+                sy = np.arange(by0, by1, dtype=np.float64)[:, None] - oy
+                if ell:
+                    m = ((sx - x0) / w) ** 2 + ((sy - y0) / h) ** 2 < 1.0
+                else:
+                    m = (sx >= x0) & (sx < x0 + w) & (sy >= y0) & (sy < y0 + h)
+                v[by0:by1, bx0:bx1][m] = pal[int(c)]
         noisy = rng.random(v.shape) < noisy_fraction
         v[noisy] += rng.normal(0.0, noise_sigma, int(noisy.sum()))
         out.append(_make_frame(v, width, height, with_chroma))
@@ -219,6 +249,15 @@ def small_clip(seed: int = 1, frames: int = 8) -> list[Frame]:
     """416x240, 8 frames: 4 sinusoids, 3 rectangles, global motion +-6 px, sigma 3."""
     return sinusoid_clip(416, 240, frames, seed, sinusoids=4, rects=3, global_motion=6.0, rect_motion=10.0,
                          noise_sigma=3.0)
+
+
+def anime_clip(seed: int = 1, frames: int = 65, width: int = 3840, height: int = 2160,
+               scene_cut: int | None = 33) -> list[Frame]:
+    """3840x2160 animation-like content: 8-24 flat colours per scene, 1-px hard edges, 0.5% of
+    pixels with noise sigma 1, piecewise-translational motion up to +-48 px, a scene cut at
+    frame 33."""
+    return animation_clip(width, height, frames, seed, colours=(8, 24), motion=48.0, noisy_fraction=0.005,
+                          noise_sigma=1.0, scene_cut=scene_cut)
 
 
 def hd_clip(seed: int = 1, frames: int = 17, width: int = 1920, height: int = 1080) -> list[Frame]:

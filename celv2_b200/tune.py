@@ -21,19 +21,26 @@ from . import engine as E
 STAGES_ME = ["me_l0", "me_l1", "me_l2", "me_l3", "me_l4"]
 
 
-def _measure(eng: E.CudaEngine, src_key: int, ref_keys, qindex: int, reps: int) -> dict:
+def _measure(eng: E.CudaEngine, run, reps: int) -> dict:
     eng.stage_times()
     for _ in range(reps):
-        eng.launch_group([src_key], [list(ref_keys)], qindex)
+        run()
     return eng.stage_times()
 
 
 def autotune(eng: E.CudaEngine, src_key: int, ref_keys, qindex: int = 130, reps: int = 3) -> dict:
     """Times every combination on the job (src_key, ref_keys) and sets the fastest per stage."""
+    return autotune_run(eng, lambda: eng.launch_group([src_key], [list(ref_keys)], qindex), reps)
+
+
+def autotune_run(eng: E.CudaEngine, run, reps: int = 3) -> dict:
+    """Times every combination on the work `run` launches -- a group of eng's, or a batch of several
+    engines whose first job is eng's (celv2_launch_multi runs the stages with its first engine's
+    configuration) -- and sets eng's fastest per stage."""
     eng.set_config(E.CFG_GRAPHS, 0)
     eng.set_config(E.CFG_PERSISTENT, 1)
     eng.stage_timing(True)
-    eng.launch_group([src_key], [list(ref_keys)], qindex)  # warm-up
+    run()  # warm-up
     results = []
     try:
         for cells, persistent, chunk in itertools.product((16, 32), (0, 1), (32, 64)):
@@ -41,7 +48,7 @@ def autotune(eng: E.CudaEngine, src_key: int, ref_keys, qindex: int = 130, reps:
                 eng.set_config(E.CFG_ME_CELLS_L0 + l, cells)
             eng.set_config(E.CFG_PERSISTENT_OFF, 0 if persistent else 0x1FF)
             eng.set_config(E.CFG_INTER_CHUNK, chunk)
-            results.append(((cells, persistent, chunk), _measure(eng, src_key, ref_keys, qindex, reps)))
+            results.append(((cells, persistent, chunk), _measure(eng, run, reps)))
     finally:
         eng.stage_timing(False)
 
