@@ -56,11 +56,12 @@ struct FrameJob {
   celv2_sb_out* out;       // [sb]
   long long lam;           // lambda_q8
   // Work counters for the roofline (null unless stage timing is on): [l] searched centres at
-  // level l, [5] distinct MVs summed over (superblock, reference), [6] compound 4x4 tiles.
+  // level l, [5] inter tile SATDs (tiles x distinct MVs per region), [6] compound 4x4 tiles.
   unsigned long long* stats;
-  // Pruning (null: the exhaustive search): per superblock, bit r keeps reference r, bit 7 keeps
-  // the intra modes (see keep_mask). The kept options are scored exactly as without pruning.
-  const uint8_t* keep;
+  // Pruning (null: the exhaustive search): per superblock a keep word (include/celv2_decision.h:
+  // references, intra, block levels, intra modes; see keep_mask). The kept options are scored
+  // exactly as without pruning.
+  const uint32_t* keep;
   long long* sb_cost;      // [sb]: the chosen partition's cost (null: not written)
 };
 
@@ -68,14 +69,23 @@ enum { kStatInterMvs = 5, kStatCompoundTiles = 6, kStats = 8 };
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// The effective keep mask of superblock sb: all options without pruning; otherwise the given
-// references (all of them if none is given in an inter frame) and, in inter frames, the intra
-// modes if bit 7 is set (a KEY frame always scores intra).
+// The effective keep word of superblock sb: all options without pruning or in a KEY frame;
+// otherwise the given references (all of them if none is given), intra if its bit is set, the
+// given block levels and intra modes (all of them if none is given).
 __device__ __forceinline__ unsigned keep_mask(const FrameJob& job, int sb) {
   const unsigned all = (1u << job.nrefs) - 1u;
-  if (!job.keep || job.nrefs == 0) return all | 0x80u;
+  if (!job.keep || job.nrefs == 0) return all | CELV2_KEEP_INTRA | CELV2_KEEP_LEVELS | CELV2_KEEP_MODES;
   const unsigned k = job.keep[sb];
-  return ((k & all) ? (k & all) : all) | (k & 0x80u);
+  const unsigned levels = k & CELV2_KEEP_LEVELS, modes = k & CELV2_KEEP_MODES;
+  return ((k & all) ? (k & all) : all) | (k & CELV2_KEEP_INTRA) | (levels ? levels : CELV2_KEEP_LEVELS) |
+         (modes ? modes : CELV2_KEEP_MODES);
+}
+
+// The square level of candidate block b: 0 for 64x64 (and its halves), 1 for 32x32, 2 for 16x16,
+// 3 for 8x8.
+__host__ __device__ __forceinline__ int block_level(int b) {
+  const int sq = b / 5;
+  return sq >= 21 ? 3 : sq >= 5 ? 2 : sq >= 1 ? 1 : 0;
 }
 
 // Whether level-0 cell (cx, cy) of reference r is read by the inter stage of a superblock that

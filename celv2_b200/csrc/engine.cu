@@ -187,8 +187,8 @@ struct NetJob {
   bool net = false;
   const float* params = nullptr;
   const void* wb = nullptr;  // bf16 weight copies of the inference kernel
-  uint8_t* keep = nullptr;
-  float tr = 0, ti = 0, band = 0;
+  uint32_t* keep = nullptr;
+  PrunerThresholds th{};
 };
 
 // Per-frame device buffers of a decision.
@@ -198,7 +198,7 @@ struct JobBuffers {
   int2* inter = nullptr;     // nsb * kMaxRefs * kBlocks
   celv2_sb_out* out = nullptr;
   celv2_sb_out* out2 = nullptr;  // group buffers: the records of every other group (see group_parity)
-  uint8_t* keep = nullptr;       // pruning masks of the job, when given (nsb)
+  uint32_t* keep = nullptr;      // pruning keep words of the job, when given (nsb)
   long long* sb_cost = nullptr;  // per superblock, the chosen partition's cost (nsb)
   float* feats = nullptr;        // the learned pruner's features (nsb x CELV2_PRUNER_FEATURES)
   bool owns_feats = false;       // group slots share one block (consecutive slots, consecutive rows)
@@ -224,7 +224,7 @@ struct celv2_engine {
   // caller memory for the next launch's records (celv2_set_output), per job; where the last
   // launch's records went (launch: last_out; group: group_out[job])
   celv2_sb_out* next_out[kMaxJobs] = {};
-  std::vector<uint8_t> next_keep[kMaxJobs];  // pruning masks for the next launch's jobs (celv2_set_keep)
+  std::vector<uint32_t> next_keep[kMaxJobs];  // keep words for the next launch's jobs (celv2_set_keep)
   celv2_sb_out* last_out = nullptr;
   celv2_sb_out* group_out[kMaxJobs] = {};
   std::vector<cudaEvent_t> row_done;
@@ -275,7 +275,7 @@ struct celv2_engine {
   bool features_on = false;
   float* pruner_params = nullptr;  // device, CELV2_PRUNER_PARAMS floats
   void* nn_wb = nullptr;           // device, bf16 weight copies for the inference kernel
-  float pruner_tr = 0.5f, pruner_ti = 0.5f, pruner_band = 0.f;
+  PrunerThresholds pruner_th{0.5f, 0.5f, 0.5f, 0.5f, 0.f};
 
   // The pruner work of a job of this engine (buffers b; keep_given: celv2_set_keep masks win).
   NetJob net_for(const FrameJob& job, const JobBuffers& b, bool keep_given) const {
@@ -284,7 +284,7 @@ struct celv2_engine {
     const bool net = pruner_params && !keep_given;
     if (!features_on && !net) return n;
     n.feats = b.feats, n.net = net, n.params = pruner_params, n.wb = nn_wb, n.keep = b.keep;
-    n.tr = pruner_tr, n.ti = pruner_ti, n.band = pruner_band;
+    n.th = pruner_th;
     return n;
   }
   int inter_chunk = 64;
@@ -382,7 +382,7 @@ struct celv2_engine {
     CK(cudaMalloc(&b.inter, (size_t)g.nsb * kMaxRefs * kBlocks * sizeof(int2)));
     CK(cudaMalloc(&b.out, (size_t)g.nsb * sizeof(celv2_sb_out)));
     if (with_intra) CK(cudaMalloc(&b.out2, (size_t)g.nsb * sizeof(celv2_sb_out)));
-    CK(cudaMalloc(&b.keep, (size_t)g.nsb));
+    CK(cudaMalloc(&b.keep, (size_t)g.nsb * sizeof(uint32_t)));
     CK(cudaMalloc(&b.sb_cost, (size_t)g.nsb * sizeof(long long)));
     if (!with_intra) {  // the group slots' features are one block (reserve_group)
       CK(cudaMalloc(&b.feats, (size_t)g.nsb * CELV2_PRUNER_FEATURES * sizeof(float)));
@@ -554,19 +554,20 @@ struct celv2_engine {
     job.sb_cost = b.sb_cost;
   }
 
-  // The pruning masks named for the next launch's jobs (celv2_set_keep); clears them.
-  std::array<std::vector<uint8_t>, kMaxJobs> take_keeps() {
-    std::array<std::vector<uint8_t>, kMaxJobs> k;
+  // The keep words named for the next launch's jobs (celv2_set_keep); clears them.
+  std::array<std::vector<uint32_t>, kMaxJobs> take_keeps() {
+    std::array<std::vector<uint32_t>, kMaxJobs> k;
     for (int j = 0; j < kMaxJobs; j++) k[j].swap(next_keep[j]);
     return k;
   }
 
   // A job's masks copied into b.keep on `stream` through the staging ring; null when none.
-  const uint8_t* put_keep(const std::vector<uint8_t>& k, const JobBuffers& b, cudaStream_t stream) {
+  const uint32_t* put_keep(const std::vector<uint32_t>& k, const JobBuffers& b, cudaStream_t stream) {
     if (k.empty()) return nullptr;
-    Stage& sg = take_stage(g.nsb);
-    std::memcpy(sg.host, k.data(), g.nsb);
-    CK(cudaMemcpyAsync(b.keep, sg.host, g.nsb, cudaMemcpyHostToDevice, stream));
+    const size_t bytes = (size_t)g.nsb * sizeof(uint32_t);
+    Stage& sg = take_stage(bytes);
+    std::memcpy(sg.host, k.data(), bytes);
+    CK(cudaMemcpyAsync(b.keep, sg.host, bytes, cudaMemcpyHostToDevice, stream));
     CK(cudaEventRecord(sg.done, stream));
     sg.pending = true;
     return b.keep;
@@ -644,7 +645,7 @@ struct celv2_engine {
       launch_features(djobs + j, nsb, nj.feats, stream);
       launched++;
       if (nj.net) {
-        launch_infer(nj.params, nj.wb, nj.feats, nsb, jobs[j].nrefs, nj.tr, nj.ti, nj.band, nj.keep, stream);
+        launch_infer(nj.params, nj.wb, nj.feats, nsb, jobs[j].nrefs, nj.th, nj.keep, stream);
         launched++;
       }
     }
@@ -673,7 +674,7 @@ struct celv2_engine {
               long long src_key) {
     celv2_sb_out* dest = take_outputs()[0];  // this launch's, even when it fails
     if (!dest) dest = host_out;
-    const std::vector<uint8_t> keep0 = std::move(take_keeps()[0]);
+    const std::vector<uint32_t> keep0 = std::move(take_keeps()[0]);
     check_frame(src, "source");
     if (nrefs < 0 || nrefs > kMaxRefs) invalid("CudaEngine: too many references");
     for (int r = 0; r < nrefs; r++) check_frame(&refs[r], "reference");
@@ -866,7 +867,7 @@ struct celv2_engine {
   void launch_group(int njobs, const long long* src_keys, const int* nrefs, const long long* const* ref_keys,
                     const int64_t* lams, bool to_host) {
     const std::array<celv2_sb_out*, kMaxJobs> dests = take_outputs();
-    const std::array<std::vector<uint8_t>, kMaxJobs> keeps = take_keeps();
+    const std::array<std::vector<uint32_t>, kMaxJobs> keeps = take_keeps();
     if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per group");
     if (!to_host)
       for (int j = 0; j < njobs; j++)
@@ -997,7 +998,7 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     if (engines[j] && std::find(uniq.begin(), uniq.end(), engines[j]) == uniq.end()) uniq.push_back(engines[j]);
   // the caller memory named for this launch, which takes it even when it fails
   std::vector<std::array<celv2_sb_out*, kMaxJobs>> dests;
-  std::vector<std::array<std::vector<uint8_t>, kMaxJobs>> keeps;
+  std::vector<std::array<std::vector<uint32_t>, kMaxJobs>> keeps;
   for (celv2_engine* e : uniq) dests.push_back(e->take_outputs()), keeps.push_back(e->take_keeps());
   if (njobs <= 0 || njobs > kMaxJobs - 1) invalid("1..31 jobs per batch");
   for (int j = 0; j < njobs; j++) {
@@ -1275,6 +1276,17 @@ int celv2_set_keep(celv2_engine* e, int job, const uint8_t* keep) {
     if (!e) invalid("null engine");
     if (job < 0 || job >= kMaxJobs - 1) invalid("set_keep: job out of range");
     if (keep)
+      e->next_keep[job].assign(keep, keep + e->g.nsb);  // references and intra; every level and mode
+    else
+      e->next_keep[job].clear();
+  });
+}
+
+int celv2_set_keep_words(celv2_engine* e, int job, const uint32_t* keep) {
+  return guarded([&] {
+    if (!e) invalid("null engine");
+    if (job < 0 || job >= kMaxJobs - 1) invalid("set_keep_words: job out of range");
+    if (keep)
       e->next_keep[job].assign(keep, keep + e->g.nsb);
     else
       e->next_keep[job].clear();
@@ -1375,10 +1387,12 @@ int celv2_debug_inter(celv2_engine* e, int32_t* out) {
 
 long long celv2_kernel_launches(const celv2_engine* e) { return e ? e->kernel_launches : 0; }
 
-int celv2_set_pruner(celv2_engine* e, const float* params, float ref_threshold, float intra_threshold, float band) {
+int celv2_set_pruner(celv2_engine* e, const float* params, float ref_threshold, float intra_threshold,
+                     float level_threshold, float mode_threshold, float band) {
   return guarded([&] {
     if (!e) invalid("null engine");
-    if (params && !(ref_threshold >= 0.f && ref_threshold <= 1.f && intra_threshold >= 0.f && intra_threshold <= 1.f &&
+    auto unit = [](float v) { return v >= 0.f && v <= 1.f; };
+    if (params && !(unit(ref_threshold) && unit(intra_threshold) && unit(level_threshold) && unit(mode_threshold) &&
                     band >= 0.f))
       invalid("set_pruner: thresholds must lie in [0, 1] and the band be >= 0");
     CK(cudaSetDevice(e->device));
@@ -1398,7 +1412,7 @@ int celv2_set_pruner(celv2_engine* e, const float* params, float ref_threshold, 
     CK(cudaMemcpyAsync(e->pruner_params, params, CELV2_PRUNER_PARAMS * sizeof(float), cudaMemcpyHostToDevice, e->st));
     infer_weights(e->pruner_params, e->nn_wb, e->st);
     CK(cudaStreamSynchronize(e->st));
-    e->pruner_tr = ref_threshold, e->pruner_ti = intra_threshold, e->pruner_band = band;
+    e->pruner_th = PrunerThresholds{ref_threshold, intra_threshold, level_threshold, mode_threshold, band};
   });
 }
 
@@ -1421,13 +1435,13 @@ int celv2_features(celv2_engine* e, int job, float* out) {
   });
 }
 
-int celv2_pruner_masks(celv2_engine* e, int job, uint8_t* out) {
+int celv2_pruner_masks(celv2_engine* e, int job, uint32_t* out) {
   return guarded([&] {
     if (!e || !out) invalid("null argument");
     const JobBuffers& b = last_buffers(e, job);
     CK(cudaSetDevice(e->device));
     e->wait_idle();
-    CK(cudaMemcpy(out, b.keep, (size_t)e->g.nsb, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(out, b.keep, (size_t)e->g.nsb * sizeof(uint32_t), cudaMemcpyDeviceToHost));
   });
 }
 

@@ -52,7 +52,8 @@ __global__ void __launch_bounds__(kFinThreads, 4) k_finalize(const FrameJob* __r
   const long long lam = job.lam;
   celv2_sb_out* o = job.out + sb;
   const int2* inter = job.inter + (long long)sb * kMaxRefs * kBlocks;
-  const unsigned keep = keep_mask(job, sb);  // pruned references and intra are not candidates
+  // pruned references, intra, block levels and intra modes are not candidates
+  const unsigned keep = keep_mask(job, sb);
 
   // 1. each reference's best, the best two references, the records per reference
   unsigned comp_tiles = 0;  // work counter: compound 4x4 tiles
@@ -60,8 +61,9 @@ __global__ void __launch_bounds__(kFinThreads, 4) k_finalize(const FrameJob* __r
     long long rc[kMaxRefs];
     int rmv[kMaxRefs];
     int a = -1, second = -1;
+    const bool live = keep & CELV2_KEEP_LEVEL(block_level(b));  // a block of a pruned level: no choice
     for (int r = 0; r < nrefs; r++) {
-      if (!(keep >> r & 1u)) {
+      if (!live || !(keep >> r & 1u)) {
         rc[r] = kMax, rmv[r] = 0;
         continue;
       }
@@ -71,10 +73,10 @@ __global__ void __launch_bounds__(kFinThreads, 4) k_finalize(const FrameJob* __r
       if (a < 0 || rc[r] < rc[a]) a = r;
     }
     for (int r = 0; r < nrefs; r++)
-      if (r != a && (keep >> r & 1u) && (second < 0 || rc[r] < rc[second])) second = r;
+      if (r != a && live && (keep >> r & 1u) && (second < 0 || rc[r] < rc[second])) second = r;
 #pragma unroll
     for (int r = 0; r < kMaxRefs; r++) {
-      const bool has = r < nrefs && (keep >> r & 1u);
+      const bool has = r < nrefs && live && (keep >> r & 1u);
       const long long c8 = has ? rc[r] >> 8 : 0;
       o->c_rcost[r][b] = has ? (unsigned)(c8 < 0xfffffffeLL ? c8 : 0xfffffffeLL) : CELV2_NO_REF_COST;
       o->c_rmvx[r][b] = (short)(has ? mv_x(rmv[r]) : 0);
@@ -158,8 +160,10 @@ __global__ void __launch_bounds__(kFinThreads, 4) k_finalize(const FrameJob* __r
     }
     long long c = kMax;
     int m = 0;
-    if (b >= 5 && (keep & 0x80u))
+    const bool live = keep & CELV2_KEEP_LEVEL(block_level(b));
+    if (b >= 5 && live && (keep & CELV2_KEEP_INTRA))
       for (int k = 0; k < kModes; k++) {
+        if (!(keep & CELV2_KEEP_MODE(k))) continue;
         const long long ck = (long long)intra[b * kModes + k] * 256 + lam * (mode_bits(k) + (nrefs > 0 ? kIntraInInterBits : 0));
         if (ck < c) c = ck, m = k;
       }
@@ -170,7 +174,7 @@ __global__ void __launch_bounds__(kFinThreads, 4) k_finalize(const FrameJob* __r
     o->c_ref[b] = (unsigned char)ref, o->c_ref2[b] = (unsigned char)ref2;
     o->c_mv2x[b] = (short)mv_x(mv2), o->c_mv2y[b] = (short)mv_y(mv2);
     const bool take_inter = ci < c;
-    S.best_cost[b] = take_inter ? ci : c;
+    S.best_cost[b] = live ? (take_inter ? ci : c) : CELV2_PRUNED_COST;
     S.best_mode[b] = take_inter ? kModes : m;
     S.best_mv[b] = take_inter ? mv : 0;
     S.best_ref[b] = take_inter ? ref : 0;

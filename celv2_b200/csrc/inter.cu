@@ -21,6 +21,11 @@
 //     first strict minimum over the candidates in order: a repeated MV (which the reference skips)
 //     has the same SATD as its first occurrence and a larger index, so it never wins.
 // 256 |D| Hadamards per (superblock, reference) instead of up to 68,352 for the blocks one by one.
+// Pruned search: where the superblock keeps no 64-level blocks (no 64x64, 64x32, 32x64), each of
+// its 32x32 regions (16x16 with no 32-level blocks either) is scored on its own: a kept block and
+// all its candidates' cells lie inside its region and the ring of cells around it, so the region's
+// tiles are scored at the distinct MVs of its 6 x 6 (4 x 4) cells only -- exactly the SATDs the
+// whole-superblock pass gives them.
 // The result per (block, reference) is the winning SATD and MV; the lambda terms are added by the
 // finalize stage, which alone needs the costs.
 #include <algorithm>
@@ -42,19 +47,22 @@ __device__ unsigned g_slot[kSlots];
 __constant__ short c_cand_off[kBlocks];
 __device__ unsigned char g_cand_cell[kSlots];
 
+constexpr int kMaxRegions = 16;  // 16x16 regions of a superblock
+constexpr int kRegCells = 256;   // regions x neighbourhood cells at most (16 x 16, 4 x 36, 1 x 100)
+
 struct InterSmem {
-  int nb[kNb];  // packed MV of each neighbourhood cell
-  int D[kNb];   // distinct MVs, first occurrence order
-  int first_idx[kNb];
-  unsigned char dmap[kNb];
-  int moff[kNb];  // per MV of D: the superblock's prediction, bytes from the reference's level 0
-  unsigned char mfast[kNb];           // per MV of D: its 64 x 64 prediction lies inside the margin
-  unsigned char list[kSlots];         // per candidate slot: its MV index in D
+  int nb[kNb];                 // packed MV of each neighbourhood cell
+  int D[kRegCells];            // per region r: its distinct MVs at D[r * ncell ..], first occurrence order
+  int moff[kRegCells];         // per (region, MV): the superblock's prediction, bytes from the reference's level 0
+  unsigned char mfast[kRegCells];  // per (region, MV): the region's prediction lies inside the margin
+  unsigned char first[kRegCells];  // per (region, cell): the cell holds the first occurrence of its MV
+  unsigned char dmap[kMaxRegions][kNb];  // per region: neighbourhood cell -> its MV's index in the region's D
+  int nd[kMaxRegions];
+  unsigned char list[kSlots];         // per candidate slot: its MV index in its region's D (255: pruned block)
   unsigned key[kBlocks];              // per block: least (SATD << 7 | candidate index) so far
   unsigned short tile[kChunk][256];   // 4x4 SATDs (at most 16 x 4 x 255 = 16,320)
   unsigned short whole8[kChunk][64];  // 8x8 sums (at most 65,280)
   int sum16[kChunk][16];
-  int nd;
 };
 
 // SATD of block b at chunk-local MV dd from the shared sums.
@@ -130,7 +138,6 @@ __host__ __device__ __forceinline__ int candidate_cell(int bx, int by, int bw, i
 __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __restrict__ jobs, WorkList w, int chunk) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   InterSmem& S = *reinterpret_cast<InterSmem*>(smem_raw);
-  __shared__ int warp_cnt[kInterThreads / 32];
   __shared__ int unit_slot;
   const int tid = threadIdx.x, lane = tid & 31;
   int unit, iter = 0;
@@ -140,12 +147,17 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   const int nsb = job.sb_cols * job.sb_rows;
   const int u = unit - w.prefix[jb];
   const int r = u / nsb, sb = u - r * nsb, sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
-  if (!(keep_mask(job, sb) >> r & 1u)) continue;  // a pruned (superblock, reference): not scored
+  const unsigned keep = keep_mask(job, sb);
+  if (!(keep >> r & 1u)) continue;  // a pruned (superblock, reference): not scored
   const int ox = sbx * 64, oy = sby * 64;
   const int cols = job.fcols[0], rows = job.frows[0];
   const int* field = job.field[r][0];
+  // regions: the whole superblock, or its 32x32 / 16x16 squares where larger blocks are pruned
+  const int R = (keep & CELV2_KEEP_LEVEL(0)) ? 64 : (keep & CELV2_KEEP_LEVEL(1)) ? 32 : 16;
+  const int nr = 64 / R, nreg = nr * nr, rc = R / 8 + 2, ncell = rc * rc;
 
-  // 1. neighbourhood MVs, their distinct set (first occurrence order), the blocks' lists
+  // 1. neighbourhood MVs; per region the distinct MVs of its cells (first occurrence order) and
+  //    the map from its cells to them; the blocks' candidate lists
   if (tid < kNb) {
     const int ny = tid / 10, nx = tid - ny * 10;
     const int cx = clampi(sbx * 8 - 1 + nx, 0, cols - 1), cy = clampi(sby * 8 - 1 + ny, 0, rows - 1);
@@ -153,38 +165,52 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   }
   for (int b = tid; b < kBlocks; b += kInterThreads) S.key[b] = 0xffffffffu;
   __syncthreads();
-  bool is_first = false;
-  int firstj = 0;
-  if (tid < kNb) {
-    const int v = S.nb[tid];
-    while (S.nb[firstj] != v) firstj++;
-    is_first = firstj == tid;
+  // thread e is local cell lc of region reg: neighbourhood cell c10
+  const int e = tid, reg = e / ncell, lc = e - reg * ncell;
+  const bool elive = e < nreg * ncell;
+  const int rx0 = (reg % nr) * (R / 8), ry0 = (reg / nr) * (R / 8);
+  const int c10 = (ry0 + lc / rc) * 10 + rx0 + lc % rc;
+  int firstlc = 0;  // the region's first local cell with this cell's MV
+  if (elive) {
+    const int v = S.nb[c10];
+    while (S.nb[(ry0 + firstlc / rc) * 10 + rx0 + firstlc % rc] != v) firstlc++;
+    S.first[e] = firstlc == lc;
   }
-  const unsigned bal = __ballot_sync(0xffffffffu, is_first);
-  if (lane == 0) warp_cnt[tid >> 5] = __popc(bal);
   __syncthreads();
-  if (tid < kNb) {
-    int pos = __popc(bal & ((1u << lane) - 1u));
-    for (int k = 0; k < (tid >> 5); k++) pos += warp_cnt[k];
-    if (is_first) S.D[pos] = S.nb[tid], S.first_idx[tid] = pos;
+  if (elive) {  // the MV's index in the region's D: the first occurrences before its own
+    int pos = 0;
+    for (int k = 0; k < firstlc; k++) pos += S.first[reg * ncell + k];
+    S.dmap[reg][c10] = (unsigned char)pos;
+    if (firstlc == lc) S.D[reg * ncell + pos] = S.nb[c10];
   }
-  if (tid == 0) S.nd = warp_cnt[0] + warp_cnt[1] + warp_cnt[2] + warp_cnt[3];
+  if (tid < nreg) {
+    int n = 0;
+    for (int k = 0; k < ncell; k++) n += S.first[tid * ncell + k];
+    S.nd[tid] = n;
+  }
   __syncthreads();
-  if (tid < kNb) S.dmap[tid] = (unsigned char)S.first_idx[firstj];
-  const int nd = S.nd;
-  if (tid == 0 && job.stats) atomicAdd(job.stats + kStatInterMvs, (unsigned long long)nd);
   const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
-  if (tid < nd) {
-    const int m = S.D[tid], mx = mv_x(m), my = mv_y(m), x = ox + (mx >> 2), y = oy + (my >> 2);
+  if (elive && lc < S.nd[reg]) {  // per (region, MV): the prediction's offset, inside the margin or not
+    const int m = S.D[e], mx = mv_x(m), my = mv_y(m);
+    const int x = ox + (mx >> 2), y = oy + (my >> 2);
     const long long o = (long long)((my & 3) * 4 + (mx & 3)) * ref.phase + (long long)y * ref.stride + x;
-    S.moff[tid] = (int)o;
-    S.mfast[tid] = inside(ref, x, y, 64, 64) && o == (long long)(int)o;
+    S.moff[e] = (int)o;
+    S.mfast[e] = inside(ref, x + (reg % nr) * R, y + (reg / nr) * R, R, R) && o == (long long)(int)o;
   }
-  __syncthreads();
-  for (int e = tid; e < kSlots; e += kInterThreads) S.list[e] = S.dmap[g_slot[e] >> 16];
+  int nd_max = 0, nd_sum = 0;
+  for (int k = 0; k < nreg; k++) nd_max = max(nd_max, S.nd[k]), nd_sum += S.nd[k];
+  if (tid == 0 && job.stats) atomicAdd(job.stats + kStatInterMvs, (unsigned long long)nd_sum * (R / 4) * (R / 4));
+  for (int k = tid; k < kSlots; k += kInterThreads) {
+    const unsigned bp = g_slot[k];
+    const int b = bp & 511;
+    int bx, by, bw, bh;
+    sb_block_geom(b, bx, by, bw, bh);
+    S.list[k] = (keep & CELV2_KEEP_LEVEL(block_level(b))) ? S.dmap[(by / R) * nr + bx / R][bp >> 16] : (unsigned char)255;
+  }
 
   // this thread's tile: its cur rows, row-transformed, in registers (the grid lies inside the margin)
   const int tx = tid & 15, ty = tid >> 4;
+  const int treg = (ty / (R / 4)) * nr + tx / (R / 4);  // the tile's region
   int C[16];
   {
     uint32_t c[4];
@@ -195,21 +221,25 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   // the tile's prediction rows at MV d start at tile_base + moff[d]; words a row apart are ws apart
   const uintptr_t tile_base = reinterpret_cast<uintptr_t>(ref.p) + (uintptr_t)(ty * 4 * ref.stride + tx * 4);
   const int ws = ref.stride >> 2;  // strides are multiples of 64
-  // chunks of equal size, at most `chunk` MVs each
-  const int nchunks = (nd + chunk - 1) / chunk, csize = (nd + nchunks - 1) / nchunks;
-  __syncthreads();  // lists complete
+  __syncthreads();  // lists, offsets complete
+  const int tnd = S.nd[treg], tbase = treg * ncell;
+  // chunks of equal size, at most `chunk` MVs each (a region's MVs past its count are not scored)
+  const int nchunks = (nd_max + chunk - 1) / chunk, csize = (nd_max + nchunks - 1) / nchunks;
 
-  for (int c0 = 0; c0 < nd; c0 += csize) {
-    const int nc = min(csize, nd - c0);
+  for (int c0 = 0; c0 < nd_max; c0 += csize) {
+    const int nc = min(csize, nd_max - c0);
+    const int tnc = min(nc, tnd - c0);  // this tile's region's MVs in the chunk
     // 2. tile SATDs at every MV of the chunk (two MVs per step for load parallelism); an 8x8
-    //    cell's tiles are lanes l, l + 1, l + 16, l + 17 of one warp
+    //    cell's tiles are lanes l, l + 1, l + 16, l + 17 of one warp (and of one region)
     for (int dd = 0; dd < nc; dd += 2) {
       int sat[2];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int d = c0 + min(dd + h, nc - 1);
+        // a region with no MV left in this chunk scores its first MV (always there) and its
+        // sums are never read: its slots name only its own MVs
+        const int d = tbase + (tnc > 0 ? c0 + min(dd + h, tnc - 1) : 0);
         uint32_t pr[4];
-        if (S.mfast[d]) {  // the usual case, uniform over the CTA: rows from aligned words
+        if (S.mfast[d]) {  // the usual case: rows from aligned words
           const uintptr_t a = tile_base + (uintptr_t)(intptr_t)S.moff[d];
           const uint32_t* wp = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
           const uint32_t sh = (uint32_t)(a & 3) * 8;
@@ -245,26 +275,30 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
       }
     }
     __syncthreads();
-    for (int e = tid; e < nc * 16; e += kInterThreads) {
-      const int dd = e >> 4, i = e & 15, c = (i >> 2) * 16 + (i & 3) * 2;
+    for (int k = tid; k < nc * 16; k += kInterThreads) {
+      const int dd = k >> 4, i = k & 15, c = (i >> 2) * 16 + (i & 3) * 2;
       const unsigned short* W = S.whole8[dd];
       S.sum16[dd][i] = W[c] + W[c + 1] + W[c + 8] + W[c + 9];
     }
     __syncthreads();
-    // 3. every candidate slot whose MV is in this chunk
-    for (int e = tid; e < kSlots; e += kInterThreads) {
-      const int d = (int)S.list[e] - c0;
-      if (d < 0 || d >= nc) continue;
-      const unsigned bp = g_slot[e];
-      const int b = bp & 511, k = (bp >> 9) & 127;
-      atomicMin(&S.key[b], ((unsigned)block_satd(S, b, d) << 7) | (unsigned)k);
+    // 3. every candidate slot whose MV is in this chunk (the slot's region's MVs)
+    for (int k = tid; k < kSlots; k += kInterThreads) {
+      const int d = (int)S.list[k] - c0;
+      if (d < 0 || d >= nc) continue;  // 255: a pruned block
+      const unsigned bp = g_slot[k];
+      const int b = bp & 511, kk = (bp >> 9) & 127;
+      atomicMin(&S.key[b], ((unsigned)block_satd(S, b, d) << 7) | (unsigned)kk);
     }
     __syncthreads();  // the next chunk overwrites the sums
   }
   int2* out = job.inter + ((long long)sb * kMaxRefs + r) * kBlocks;
   for (int b = tid; b < kBlocks; b += kInterThreads) {
+    if (!(keep & CELV2_KEEP_LEVEL(block_level(b)))) continue;  // a pruned block: never read
+    int bx, by, bw, bh;
+    sb_block_geom(b, bx, by, bw, bh);
+    const int breg = (by / R) * nr + bx / R;
     const unsigned k = S.key[b];
-    out[b] = make_int2((int)(k >> 7), S.D[S.dmap[g_cand_cell[c_cand_off[b] + (k & 127)]]]);
+    out[b] = make_int2((int)(k >> 7), S.D[breg * ncell + S.dmap[breg][g_cand_cell[c_cand_off[b] + (k & 127)]]]);
   }
   }  // units
 }

@@ -76,14 +76,20 @@ void launch_finalize(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
 // forward pass into a cache of batch x CELV2_PRUNER_ACTS floats (logits last), and the masks.
 void launch_features(const FrameJob* djob, int nsb, float* out, cudaStream_t st);
 void pruner_forward(const float* params, const float* x, int batch, float* acts, cudaStream_t st);
-void launch_masks(const float* logits, int nsb, int nrefs, float tr, float ti, float band, uint8_t* keep,
+// The pruner's decision rule: per output group the probability a kept option needs (references,
+// intra, block levels, intra modes), and the band around them inside which a superblock falls back
+// to the full search.
+struct PrunerThresholds {
+  float ref, intra, level, mode, band;
+};
+void launch_masks(const float* logits, int nsb, int nrefs, const PrunerThresholds& th, uint32_t* keep,
                   cudaStream_t st);
 // The engine's inference: the network and the mask of every superblock of one job in one kernel,
 // from bf16 weight copies (infer_weights: infer_weight_elems() bf16 elements).
 size_t infer_weight_elems();
 void infer_weights(const float* params, void* wb, cudaStream_t st);
-void launch_infer(const float* params, const void* wb, const float* feats, int nsb, int nrefs, float tr, float ti,
-                  float band, uint8_t* keep, cudaStream_t st);
+void launch_infer(const float* params, const void* wb, const float* feats, int nsb, int nrefs,
+                  const PrunerThresholds& th, uint32_t* keep, cudaStream_t st);
 
 // Set-up of the constant tables (once per device).
 cudaError_t init_tables();

@@ -22,11 +22,11 @@ namespace nn {
 constexpr int kF = CELV2_PRUNER_FEATURES, kOut = CELV2_PRUNER_OUTPUTS;
 // parameter offsets
 constexpr int kW1 = 0, kB1 = kW1 + 16 * 9, kW2 = kB1 + 16, kB2 = kW2 + 32 * 144, kW3 = kB2 + 32, kB3 = kW3 + 32 * 288,
-              kW4 = kB3 + 32, kB4 = kW4 + 64 * 632, kW5 = kB4 + 64, kB5 = kW5 + 8 * 64, kParams = kB5 + 8;
+              kW4 = kB3 + 32, kB4 = kW4 + 64 * 632, kW5 = kB4 + 64, kB5 = kW5 + kOut * 64, kParams = kB5 + kOut;
 static_assert(kParams == CELV2_PRUNER_PARAMS, "parameter count");
 // forward cache, floats per sample, in this order
 constexpr int kCols1 = 256 * 9, kA1 = 256 * 16, kCols2 = 64 * 144, kA2 = 64 * 32, kCols3 = 16 * 288, kA3 = 16 * 32,
-              kH0 = 632, kA4 = 64, kLogits = 8;
+              kH0 = 632, kA4 = 64, kLogits = kOut;
 static_assert(kCols1 + kA1 + kCols2 + kA2 + kCols3 + kA3 + kH0 + kA4 + kLogits == CELV2_PRUNER_ACTS, "cache size");
 // backward workspace, floats per sample
 constexpr int kDz4 = 64, kDh0 = 512, kDcols3 = 4608, kDz2 = 2048, kDcols2 = 9216, kDz1 = 4096;
@@ -262,7 +262,7 @@ void forward(const float* P, const float* x, int batch, float* acts, cudaStream_
   cudaMemsetAsync(c.a4, 0, (size_t)b * kA4 * sizeof(float), st);
   gemm(batch, 64, 632, c.h0, 632, 1, P + kW4, 1, 632, c.a4, 64, 1, P + kB4, false, false, st, 8);
   k_relu<<<grid_for(b * kA4), 256, 0, st>>>(c.a4, b * kA4);
-  gemm(batch, 8, 64, c.a4, 64, 1, P + kW5, 1, 64, c.logits, 8, 1, P + kB5, false, false, st);
+  gemm(batch, kOut, 64, c.a4, 64, 1, P + kW5, 1, 64, c.logits, kOut, 1, P + kB5, false, false, st);
 }
 
 void backward(const float* P, int batch, const float* acts, const float* dlogits, float* work, float* G,
@@ -276,10 +276,10 @@ void backward(const float* P, int batch, const float* acts, const float* dlogits
   float* dcols2 = dz2 + b * kDz2;
   float* dz1 = dcols2 + b * kDcols2;
   cudaMemsetAsync(G, 0, kParams * sizeof(float), st);  // the bias sums accumulate
-  // dense 64 -> 8
-  gemm(8, 64, batch, dlogits, 1, 8, c.a4, 64, 1, G + kW5, 64, 1, nullptr, false, false, st, wsplit(b));
-  k_colsum<<<grid_for(b), 64, 0, st>>>(dlogits, b, 8, G + kB5);
-  gemm(batch, 64, 8, dlogits, 8, 1, P + kW5, 64, 1, dz4, 64, 1, nullptr, false, false, st);
+  // dense 64 -> kOut
+  gemm(kOut, 64, batch, dlogits, 1, kOut, c.a4, 64, 1, G + kW5, 64, 1, nullptr, false, false, st, wsplit(b));
+  k_colsum<<<grid_for(b), 64, 0, st>>>(dlogits, b, kOut, G + kB5);
+  gemm(batch, 64, kOut, dlogits, kOut, 1, P + kW5, 64, 1, dz4, 64, 1, nullptr, false, false, st);
   k_relu_bwd<<<grid_for(b * 64), 256, 0, st>>>(c.a4, dz4, dz4, b * 64);
   // dense 632 -> 64 (the gradient reaches only the convolution part of its input)
   gemm(64, 632, batch, dz4, 1, 64, c.h0, 632, 1, G + kW4, 632, 1, nullptr, false, false, st, wsplit(b));
@@ -350,33 +350,52 @@ void launch_features(const FrameJob* djob, int nsb, float* out, cudaStream_t st)
   k_features<<<nsb, 128, 0, st>>>(djob, out);
 }
 
-// keep[sb] from the logits: reference r kept where sigmoid >= tr (the likeliest always), intra where
-// sigmoid >= ti; everything where some output lies within `band` of its threshold.
-__global__ void k_masks(const float* __restrict__ logits, int nsb, int nrefs, float tr, float ti, float band,
-                        uint8_t* __restrict__ keep) {
-  const int sb = blockIdx.x * blockDim.x + threadIdx.x;
-  if (sb >= nsb) return;
-  const float* z = logits + (long long)sb * nn::kOut;
+// The keep word (include/celv2_decision.h) of one superblock from its logits: reference r kept
+// where sigmoid >= th.ref (the likeliest reference always), intra where >= th.intra, block level l
+// where >= th.level (the likeliest level always), and with intra the modes DC, V, H (their scoring
+// costs next to nothing) and each other mode m where >= th.mode; everything where one of the
+// reference, intra or level outputs lies within th.band of its threshold (the fallback to the full
+// search).
+__device__ __forceinline__ uint32_t mask_word(const float* z, int nrefs, const PrunerThresholds& th) {
   unsigned k = 0;
-  int best = 0;
-  float pbest = -1.f;
+  int best = 0, lbest = 0;
+  float pbest = -1.f, plbest = -1.f;
   bool unsure = false;
   for (int r = 0; r < nrefs; r++) {
     const float p = 1.f / (1.f + expf(-z[r]));
-    if (p >= tr) k |= 1u << r;
+    if (p >= th.ref) k |= 1u << r;
     if (p > pbest) pbest = p, best = r;
-    unsure |= fabsf(p - tr) < band;
+    unsure |= fabsf(p - th.ref) < th.band;
   }
-  const float pi = 1.f / (1.f + expf(-z[7]));
-  if (pi >= ti) k |= 0x80u;
-  unsure |= fabsf(pi - ti) < band;
   k |= 1u << best;
-  keep[sb] = (uint8_t)(unsure ? 0xFFu : k);
+  const float pi = 1.f / (1.f + expf(-z[7]));
+  if (pi >= th.intra) k |= CELV2_KEEP_INTRA;
+  unsure |= fabsf(pi - th.intra) < th.band;
+  for (int l = 0; l < 4; l++) {
+    const float p = 1.f / (1.f + expf(-z[8 + l]));
+    if (p >= th.level) k |= CELV2_KEEP_LEVEL(l);
+    if (p > plbest) plbest = p, lbest = l;
+    unsure |= fabsf(p - th.level) < th.band;
+  }
+  k |= CELV2_KEEP_LEVEL(lbest);
+  if (k & CELV2_KEEP_INTRA) {
+    k |= CELV2_KEEP_MODE(0) | CELV2_KEEP_MODE(1) | CELV2_KEEP_MODE(2);
+    for (int m = 3; m < kModes; m++)
+      if (1.f / (1.f + expf(-z[12 + m - 3])) >= th.mode) k |= CELV2_KEEP_MODE(m);
+  }
+  return unsure ? 0xFFFFFFFFu : k;
 }
 
-void launch_masks(const float* logits, int nsb, int nrefs, float tr, float ti, float band, uint8_t* keep,
+__global__ void k_masks(const float* __restrict__ logits, int nsb, int nrefs, PrunerThresholds th,
+                        uint32_t* __restrict__ keep) {
+  const int sb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sb >= nsb) return;
+  keep[sb] = mask_word(logits + (long long)sb * nn::kOut, nrefs, th);
+}
+
+void launch_masks(const float* logits, int nsb, int nrefs, const PrunerThresholds& th, uint32_t* keep,
                   cudaStream_t st) {
-  k_masks<<<(nsb + 127) / 128, 128, 0, st>>>(logits, nsb, nrefs, tr, ti, band, keep);
+  k_masks<<<(nsb + 127) / 128, 128, 0, st>>>(logits, nsb, nrefs, th, keep);
 }
 
 void pruner_forward(const float* params, const float* x, int batch, float* acts, cudaStream_t st) {
@@ -415,8 +434,8 @@ __device__ __forceinline__ void mma16816(float* d, const uint32_t* a, uint32_t b
 }
 
 __global__ void __launch_bounds__(128) k_infer(const float* __restrict__ P, const __nv_bfloat16* __restrict__ Wb,
-                                               const float* __restrict__ feats, int nrefs, float tr, float ti,
-                                               float band, uint8_t* __restrict__ keep) {
+                                               const float* __restrict__ feats, int nrefs, PrunerThresholds th,
+                                               uint32_t* __restrict__ keep) {
   __shared__ float xr[kF];                            // the features, bf16-rounded
   __shared__ __align__(16) __nv_bfloat16 a1[256][16];  // conv1 output, (y, x) rows, channels
   __shared__ __align__(16) __nv_bfloat16 a2[64][32];
@@ -502,30 +521,14 @@ __global__ void __launch_bounds__(128) k_infer(const float* __restrict__ P, cons
   __syncthreads();
   if (tid < 64) a4[tid] = rbf(fmaxf(part[tid] + part[tid + 64] + P[kB4 + tid], 0.f));
   __syncthreads();
-  // dense 64 -> 8: warp w, lanes sum over the 64 inputs for outputs 2w, 2w + 1
-  for (int o = warp * 2; o < warp * 2 + 2; o++) {
+  // dense 64 -> kOut: warp w, lanes sum over the 64 inputs for outputs w, w + 4, ...
+  for (int o = warp; o < kOut; o += 4) {
     float s = a4[lane] * rbf(P[kW5 + o * 64 + lane]) + a4[lane + 32] * rbf(P[kW5 + o * 64 + lane + 32]);
     for (int d = 16; d > 0; d >>= 1) s += __shfl_xor_sync(0xffffffffu, s, d);
     if (lane == 0) logits[o] = s + P[kB5 + o];
   }
   __syncthreads();
-  if (tid == 0) {  // the mask (k_masks' rule)
-    unsigned k = 0;
-    int best = 0;
-    float pbest = -1.f;
-    bool unsure = false;
-    for (int r = 0; r < nrefs; r++) {
-      const float pr = 1.f / (1.f + expf(-logits[r]));
-      if (pr >= tr) k |= 1u << r;
-      if (pr > pbest) pbest = pr, best = r;
-      unsure |= fabsf(pr - tr) < band;
-    }
-    const float pi = 1.f / (1.f + expf(-logits[7]));
-    if (pi >= ti) k |= 0x80u;
-    unsure |= fabsf(pi - ti) < band;
-    k |= 1u << best;
-    keep[blockIdx.x] = (uint8_t)(unsure ? 0xFFu : k);
-  }
+  if (tid == 0) keep[blockIdx.x] = mask_word(logits, nrefs, th);  // k_masks' rule
 }
 }  // namespace nn
 
@@ -534,9 +537,9 @@ size_t infer_weight_elems() { return nn::kIWs; }
 void infer_weights(const float* params, void* wb, cudaStream_t st) {
   nn::k_infer_weights<<<nn::grid_for(nn::kIWs), 256, 0, st>>>(params, static_cast<__nv_bfloat16*>(wb));
 }
-void launch_infer(const float* params, const void* wb, const float* feats, int nsb, int nrefs, float tr, float ti,
-                  float band, uint8_t* keep, cudaStream_t st) {
-  nn::k_infer<<<nsb, 128, 0, st>>>(params, static_cast<const __nv_bfloat16*>(wb), feats, nrefs, tr, ti, band, keep);
+void launch_infer(const float* params, const void* wb, const float* feats, int nsb, int nrefs,
+                  const PrunerThresholds& th, uint32_t* keep, cudaStream_t st) {
+  nn::k_infer<<<nsb, 128, 0, st>>>(params, static_cast<const __nv_bfloat16*>(wb), feats, nrefs, th, keep);
 }
 
 }  // namespace celv2cu

@@ -85,7 +85,8 @@ SIGNATURES = {
                                    C.c_void_p]),
     "celv2_pruner_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float,
                                     C.c_float, C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]),
-    "celv2_set_pruner": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float]),
+    "celv2_set_pruner": (C.c_int, [C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "celv2_set_keep_words": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "celv2_features": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "celv2_pruner_masks": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "celv2_sb_costs": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int64)]),
@@ -93,7 +94,17 @@ SIGNATURES = {
 
 CFG_PERSISTENT, CFG_GRAPHS, CFG_PERSISTENT_OFF, CFG_INTER_CHUNK, CFG_FEATURES, CFG_ME_CELLS_L0 = 1, 2, 3, 4, 5, 10
 
-PRUNER_FEATURES, PRUNER_OUTPUTS, PRUNER_PARAMS, PRUNER_ACTS, PRUNER_WORK = 376, 8, 55080, 23488, 20544
+PRUNER_FEATURES, PRUNER_OUTPUTS, PRUNER_PARAMS, PRUNER_ACTS, PRUNER_WORK = 376, 24, 56120, 23504, 20544
+# keep words (include/celv2_decision.h)
+KEEP_INTRA, KEEP_LEVELS, KEEP_MODES = 0x80, 0xF00, 0x1FFF0000
+
+
+def keep_level(l: int) -> int:
+    return 0x100 << l
+
+
+def keep_mode(m: int) -> int:
+    return 0x10000 << m
 
 STAGE_NAMES = ["upload+pyramid", "phases", "me_l4", "me_l3", "me_l2", "me_l1", "me_l0", "intra", "inter",
                "finalize", "me_refine", "pruner"]
@@ -409,27 +420,31 @@ class CudaEngine:
         _check(library().celv2_set_output(self._h, job, ptr))
 
     def set_keep(self, job: int, keep) -> None:
-        """celv2_set_keep: pruning masks (one byte per superblock) for job of the next launch;
-        None: the exhaustive search."""
+        """Pruning masks for job of the next launch, one per superblock: uint8 bytes (references and
+        intra, celv2_set_keep) or uint32 keep words (references, intra, block levels, intra modes,
+        celv2_set_keep_words); None: the exhaustive search."""
         if keep is None:
-            _check(library().celv2_set_keep(self._h, job, None))
+            _check(library().celv2_set_keep_words(self._h, job, None))
             return
-        k = np.ascontiguousarray(keep, dtype=np.uint8)
+        words = np.asarray(keep).dtype != np.uint8
+        k = np.ascontiguousarray(keep, dtype=np.uint32 if words else np.uint8)
         if k.size != self.sb_cols * self.sb_rows:
-            raise ValueError("set_keep: one byte per superblock")
-        _check(library().celv2_set_keep(self._h, job, k.ctypes.data))
+            raise ValueError("set_keep: one mask per superblock")
+        fn = library().celv2_set_keep_words if words else library().celv2_set_keep
+        _check(fn(self._h, job, k.ctypes.data))
 
     def set_pruner(self, params, ref_threshold: float = 0.5, intra_threshold: float = 0.5,
-                   band: float = 0.0) -> None:
+                   level_threshold: float = 0.5, mode_threshold: float = 0.5, band: float = 0.0) -> None:
         """celv2_set_pruner: the learned pruner (FP32 parameters, CELV2_PRUNER_PARAMS) scores every
-        later inter frame on its own masks; None turns it off."""
+        later inter frame on its own keep words; None turns it off."""
         if params is None:
-            _check(library().celv2_set_pruner(self._h, None, 0.0, 0.0, 0.0))
+            _check(library().celv2_set_pruner(self._h, None, 0.0, 0.0, 0.0, 0.0, 0.0))
             return
         p = np.ascontiguousarray(params, dtype=np.float32)
         if p.size != PRUNER_PARAMS:
             raise ValueError(f"set_pruner: {PRUNER_PARAMS} parameters")
-        _check(library().celv2_set_pruner(self._h, p.ctypes.data, ref_threshold, intra_threshold, band))
+        _check(library().celv2_set_pruner(self._h, p.ctypes.data, ref_threshold, intra_threshold, level_threshold,
+                                          mode_threshold, band))
 
     def features(self, job: int = 0) -> np.ndarray:
         """The last launch's learned-pruner features of job (nsb x CELV2_PRUNER_FEATURES)."""
@@ -438,8 +453,8 @@ class CudaEngine:
         return out
 
     def pruner_masks(self, job: int = 0) -> np.ndarray:
-        """The masks the pruner chose for the last launch's job (one byte per superblock)."""
-        out = np.empty(self.sb_cols * self.sb_rows, dtype=np.uint8)
+        """The keep words the pruner chose for the last launch's job (one uint32 per superblock)."""
+        out = np.empty(self.sb_cols * self.sb_rows, dtype=np.uint32)
         _check(library().celv2_pruner_masks(self._h, job, out.ctypes.data))
         return out
 

@@ -12,11 +12,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "weights.npz")
 
 
+THRESHOLDS = ("ref_threshold", "intra_threshold", "level_threshold", "mode_threshold", "band")
+
+
 def load(path: str = WEIGHTS) -> dict:
     """The trained parameters and the thresholds chosen with them: {"params", "ref_threshold",
-    "intra_threshold", "band"}."""
+    "intra_threshold", "level_threshold", "mode_threshold", "band"}."""
     import numpy as np
 
+    from .. import engine as E
+
     z = np.load(path)
-    return {"params": z["params"].astype(np.float32), "ref_threshold": float(z["ref_threshold"]),
-            "intra_threshold": float(z["intra_threshold"]), "band": float(z["band"])}
+    if z["params"].size != E.PRUNER_PARAMS or any(k not in z for k in THRESHOLDS):
+        raise ValueError(f"{path} holds another network's weights (retrain: python -m celv2_b200.pruner.train)")
+    out = {"params": z["params"].astype(np.float32)}
+    for k in THRESHOLDS:
+        out[k] = float(z[k])
+    return out
+
+
+def set_on(eng, wts: dict) -> None:
+    """Turns the pruner on for engine `eng` with the weights and thresholds of `wts` (load())."""
+    eng.set_pruner(wts["params"], *(wts[k] for k in THRESHOLDS))

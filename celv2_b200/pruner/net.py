@@ -13,7 +13,7 @@ from .. import engine as E
 
 # (name, shape) in parameter order, as include/celv2_pruner.h lays them out
 SHAPES = [("W1", (16, 9)), ("b1", (16,)), ("W2", (32, 144)), ("b2", (32,)), ("W3", (32, 288)), ("b3", (32,)),
-          ("W4", (64, 632)), ("b4", (64,)), ("W5", (8, 64)), ("b5", (8,))]
+          ("W4", (64, 632)), ("b4", (64,)), ("W5", (E.PRUNER_OUTPUTS, 64)), ("b5", (E.PRUNER_OUTPUTS,))]
 assert sum(int(np.prod(s)) for _, s in SHAPES) == E.PRUNER_PARAMS
 
 
@@ -68,7 +68,7 @@ class Trainer:
         return self.acts[off:off + n * E.PRUNER_OUTPUTS].view(n, E.PRUNER_OUTPUTS)
 
     def step(self, x, y, w) -> None:
-        """One Adam step on the minibatch (device tensors n x FEATURES, n x 8, n x 8)."""
+        """One Adam step on the minibatch (device tensors n x FEATURES, n x OUTPUTS, n x OUTPUTS)."""
         lib = E.library()
         n = x.shape[0]
         st = self._stream()

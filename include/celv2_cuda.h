@@ -134,16 +134,21 @@ int celv2_host_alloc(long long bytes, void** out);
 int celv2_host_free(void* p);
 
 /* ---- Pruned search ----
- * No counterpart in the reference. celv2_set_keep gives the NEXT launch's job (numbered as for
- * celv2_set_output) one byte per superblock (sb_cols * sb_rows, raster order; NULL: exhaustive):
- * bit r keeps reference r, bit 7 keeps the intra modes. A superblock then scores only what it
- * keeps -- exactly as the exhaustive search scores it -- and picks among that: its pruned
- * references' records read CELV2_NO_REF_COST, and with intra pruned no block is intra. An inter
- * frame's superblock that keeps no reference keeps them all; a KEY frame always scores intra. The
- * motion search skips the level-0 cells no superblock's kept references read.
+ * No counterpart in the reference. celv2_set_keep_words gives the NEXT launch's job (numbered as
+ * for celv2_set_output) one keep word per superblock (sb_cols * sb_rows, raster order; NULL:
+ * exhaustive): the references, intra, the block levels and the intra modes it keeps
+ * (include/celv2_decision.h). A superblock then scores only what it keeps -- exactly as the
+ * exhaustive search scores it -- and picks among that: its pruned references' records read
+ * CELV2_NO_REF_COST, with intra pruned no block is intra, the blocks of a pruned level read as
+ * blocks with no choice. A KEY frame always scores everything. The motion search skips the level-0
+ * cells no superblock's kept references read; the inter stage scores only the tiles and motion
+ * vectors the kept levels' blocks use; the intra stage skips pruned levels and modes.
+ * celv2_set_keep: the same from one byte per superblock (bits 0-7 of the word: the references and
+ * intra; every level and mode kept).
  * celv2_sb_costs copies the last launch's per-superblock cost of the chosen partition (the sum the
  * partition choice minimises, lambda-weighted SATD plus rate) for one job; it waits for the work. */
 int celv2_set_keep(celv2_engine* e, int job, const uint8_t* keep);
+int celv2_set_keep_words(celv2_engine* e, int job, const uint32_t* keep);
 int celv2_sb_costs(celv2_engine* e, int job, int64_t* out);
 
 /* ---- A KEY-frame decision that allocates nothing ----
@@ -213,8 +218,9 @@ int celv2_stream(const celv2_engine* e, void** stream);
 int celv2_stage_timing(celv2_engine* e, int enable);
 int celv2_stage_times(celv2_engine* e, double* ms, long long* launches, int n);
 /* Work the kernels executed while stage timing was on, then reset: [l] motion-search centres
- * searched at level l (0..4), [5] distinct candidate MVs summed over (superblock, reference),
- * [6] compound 4x4 tiles (CELV2_WORK_COUNTERS entries). */
+ * searched at level l (0..4), [5] 4x4 tile SATDs of the inter stage (tiles x distinct candidate
+ * MVs, summed over (superblock, reference) and its regions), [6] compound 4x4 tiles
+ * (CELV2_WORK_COUNTERS entries). */
 #define CELV2_WORK_COUNTERS 8
 int celv2_work_counters(celv2_engine* e, unsigned long long* out, int n);
 /* The GPU's measured INT32 throughput (integer ops per second): the roofline denominator of the

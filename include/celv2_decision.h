@@ -49,6 +49,25 @@ typedef struct celv2_sb_out {
   int16_t c_rmvx[CELV2_MAX_REFS][CELV2_SB_BLOCKS], c_rmvy[CELV2_MAX_REFS][CELV2_SB_BLOCKS];
 } celv2_sb_out;
 
+/* Keep words of the pruned search (no counterpart in the reference, which always searches
+ * exhaustively): per superblock of an inter frame, which options the exact scorer evaluates.
+ *  bits 0-6   reference r (none set: all of them);
+ *  bit 7      the intra modes;
+ *  bits 8-11  the candidate blocks of square level l (0: 64x64, 64x32, 32x64; 1: 32x32, 32x16,
+ *             16x32; 2: 16x16, 16x8, 8x16; 3: 8x8, 8x4, 4x8) (none set: all levels);
+ *  bits 16-28 intra mode m (none set: all modes).
+ * A kept option is scored exactly as the exhaustive search scores it; a block of a pruned level is
+ * no candidate (its record reads as one with no choice: costs INT64_MAX, reference costs
+ * CELV2_NO_REF_COST) and the partition choice takes it at cost CELV2_PRUNED_COST, so that any
+ * non-empty set of levels leaves a complete partition. A KEY frame always scores everything. */
+#define CELV2_KEEP_REFS 0x7Fu
+#define CELV2_KEEP_INTRA 0x80u
+#define CELV2_KEEP_LEVEL(l) (0x100u << (l))
+#define CELV2_KEEP_LEVELS 0xF00u
+#define CELV2_KEEP_MODE(m) (0x10000u << (m))
+#define CELV2_KEEP_MODES 0x1FFF0000u
+#define CELV2_PRUNED_COST (1LL << 56)
+
 #ifdef __cplusplus
 static_assert(sizeof(celv2_sb_out) == 38872, "celv2_sb_out must keep the reference SbOut layout");
 #else

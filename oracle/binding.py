@@ -103,7 +103,7 @@ class Oracle:
         nsb = ((width + 63) // 64) * ((height + 63) // 64)
         out = np.zeros(nsb, dtype=SB_OUT_DTYPE)
         cost = np.zeros(nsb, dtype=np.int64)
-        k = None if keep is None else np.ascontiguousarray(keep, dtype=np.uint8)
+        k = None if keep is None else np.ascontiguousarray(keep, dtype=np.uint32)  # bytes: references + intra
         rc = self.lib.oro_decide_masked(_u8p(src_y), width, height, _plist(refs_y), len(refs_y), int(lam), threads,
                                         None if k is None else k.ctypes.data_as(C.c_void_p),
                                         out.ctypes.data_as(C.c_void_p), cost.ctypes.data_as(C.c_void_p))

@@ -507,12 +507,13 @@ static best_t make_best(int64_t cost, int mode, int mvx, int mvy, int ref) {
  * all first strict minimum; records the block's candidates into o[b]; returns the block's best
  * (inter only where strictly cheaper than intra). */
 static best_t block_best(const plane_t* s, const refset_t* rs, int ox, int oy, int b, int64_t lam, int intra,
-                         unsigned keep_refs, celv2_sb_out* o) {
+                         unsigned keep_refs, unsigned keep_modes, celv2_sb_out* o) {
   int bx, by, w, h;
   oro_sb_block_geom(b, &bx, &by, &w, &h);
   const int x = ox + bx, y = oy + by;
   best_t bi = make_best(INT64_MAX, 0, 0, 0, 0), be = make_best(INT64_MAX, kNumModes, 0, 0, 0);
   for (int m = 0; m < kNumModes && intra; m++) {
+    if (!(keep_modes >> m & 1u)) continue; /* a pruned mode is no candidate */
     const int64_t c = block_mode_satd(s, x, y, w, h, m) * 256 + lam * (mode_bits(m) + (rs->n > 0 ? kIntraInInterBits : 0));
     if (c < bi.cost) bi = make_best(c, m, 0, 0, 0);
   }
@@ -610,7 +611,13 @@ static void decide_sb(const plane_t* s, const refset_t* rs, int sb_col, int sb_r
       best[b] = make_best(INT64_MAX, 0, 0, 0, 0);
       continue;
     }
-    best[b] = block_best(s, rs, ox, oy, b, lam, b >= 5 && (keep & 0x80u), keep & 0x7fu, o);
+    const int sq = b / 5, level = sq >= 21 ? 3 : sq >= 5 ? 2 : sq >= 1 ? 1 : 0;
+    if (!(keep & CELV2_KEEP_LEVEL(level))) { /* a pruned level: no candidate, its record blank */
+      best[b] = make_best(CELV2_PRUNED_COST, 0, 0, 0, 0);
+      continue;
+    }
+    best[b] = block_best(s, rs, ox, oy, b, lam, b >= 5 && (keep & CELV2_KEEP_INTRA), keep & CELV2_KEEP_REFS,
+                         keep >> 16, o);
   }
   int64_t sq_cost[CELV2_SB_SQUARES];
   int choice[CELV2_SB_SQUARES];
@@ -643,17 +650,20 @@ static void decide_sb(const plane_t* s, const refset_t* rs, int sb_col, int sb_r
 }
 
 /* Pruning (an extension for testing the engine's pruned search, not a reference rule): the
- * effective mask of a superblock -- all options without masks or in a KEY frame; else the given
- * references (all if none is given) and intra if bit 7 is set. */
-static unsigned keep_of(const uint8_t* keep, int sb, int nrefs) {
+ * effective keep word of a superblock (celv2_decision.h) -- all options without masks or in a KEY
+ * frame; else the given references (all if none is given), intra if its bit is set, the given
+ * levels and intra modes (all if none is given). */
+static unsigned keep_of(const uint32_t* keep, int sb, int nrefs) {
   const unsigned all = (1u << nrefs) - 1u;
-  if (!keep || nrefs == 0) return all | 0x80u;
+  if (!keep || nrefs == 0) return all | CELV2_KEEP_INTRA | CELV2_KEEP_LEVELS | CELV2_KEEP_MODES;
   const unsigned k = keep[sb];
-  return ((k & all) ? (k & all) : all) | (k & 0x80u);
+  const unsigned levels = k & CELV2_KEEP_LEVELS, modes = k & CELV2_KEEP_MODES;
+  return ((k & all) ? (k & all) : all) | (k & CELV2_KEEP_INTRA) | (levels ? levels : CELV2_KEEP_LEVELS) |
+         (modes ? modes : CELV2_KEEP_MODES);
 }
 
 static int decide_frame(const uint8_t* src_y, int width, int height, const plane_t* ref_planes, int32_t* const* fx,
-                        int32_t* const* fy, int nrefs, int64_t lam, int threads, const uint8_t* keep,
+                        int32_t* const* fy, int nrefs, int64_t lam, int threads, const uint32_t* keep,
                         celv2_sb_out* out, int64_t* sb_cost) {
   const int pw = (width + 7) & ~7, ph = (height + 7) & ~7;
   const int sb_cols = (width + 63) / 64, sb_rows = (height + 63) / 64;
@@ -695,7 +705,7 @@ int oro_decide(const uint8_t* src_y, int width, int height, const uint8_t* const
 }
 
 int oro_decide_masked(const uint8_t* src_y, int width, int height, const uint8_t* const* ref_y, int nrefs,
-                      int64_t lambda_q8, int threads, const uint8_t* keep, celv2_sb_out* out, int64_t* sb_cost) {
+                      int64_t lambda_q8, int threads, const uint32_t* keep, celv2_sb_out* out, int64_t* sb_cost) {
   if (width <= 0 || height <= 0 || nrefs < 0 || nrefs > CELV2_MAX_REFS) return -1;
   const int pw = (width + 7) & ~7, ph = (height + 7) & ~7;
   if (nrefs == 0)

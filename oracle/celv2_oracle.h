@@ -52,12 +52,13 @@ int oro_decide(const uint8_t* src_y, int width, int height, const uint8_t* const
                int64_t lambda_q8, int threads, celv2_sb_out* out);
 
 /* oro_decide with pruning masks (an extension for testing the engine's pruned search; no
- * reference rule): keep (NULL: none) holds one byte per superblock, bit r keeping reference r and
- * bit 7 the intra modes; an inter frame's superblock that keeps no reference keeps them all, a KEY
- * frame always scores intra. A superblock scores what it keeps exactly as oro_decide does and
- * picks among it. sb_cost (NULL: not written) receives each superblock's chosen partition cost. */
+ * reference rule): keep (NULL: none) holds one keep word per superblock (celv2_decision.h: the
+ * references, intra, the block levels and the intra modes kept); a KEY frame always scores
+ * everything. A superblock scores what it keeps exactly as oro_decide does and picks among it; a
+ * block of a pruned level is no candidate and enters the partition choice at CELV2_PRUNED_COST.
+ * sb_cost (NULL: not written) receives each superblock's chosen partition cost. */
 int oro_decide_masked(const uint8_t* src_y, int width, int height, const uint8_t* const* ref_y, int nrefs,
-                      int64_t lambda_q8, int threads, const uint8_t* keep, celv2_sb_out* out, int64_t* sb_cost);
+                      int64_t lambda_q8, int threads, const uint32_t* keep, celv2_sb_out* out, int64_t* sb_cost);
 
 /* The same from prebuilt pyramids and level-0 fields (for the stage-by-stage tests). */
 int oro_decide_from_fields(const uint8_t* src_y, int width, int height, const uint8_t* const* ref_pyr,

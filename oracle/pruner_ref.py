@@ -10,9 +10,9 @@ from __future__ import annotations
 
 import numpy as np
 
-FEATURES, OUTPUTS = 376, 8
+FEATURES, OUTPUTS = 376, 24
 SHAPES = [("W1", (16, 9)), ("b1", (16,)), ("W2", (32, 144)), ("b2", (32,)), ("W3", (32, 288)), ("b3", (32,)),
-          ("W4", (64, 632)), ("b4", (64,)), ("W5", (8, 64)), ("b5", (8,))]
+          ("W4", (64, 632)), ("b4", (64,)), ("W5", (OUTPUTS, 64)), ("b5", (OUTPUTS,))]
 PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
 
 
@@ -63,7 +63,7 @@ def col2im(d: np.ndarray, B: int, H: int, W: int, C: int, s: int) -> np.ndarray:
 
 
 def forward(p: np.ndarray, x: np.ndarray, bf: bool = True):
-    """(logits [B, 8], cache)."""
+    """(logits [B, OUTPUTS], cache)."""
     dt = np.float32 if bf else np.float64
     P = {k: v.astype(dt) for k, v in unpack(p).items()}
     x = x.astype(dt)

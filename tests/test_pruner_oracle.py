@@ -17,15 +17,15 @@ def loss_of(p, x, y, w):
 
 
 def test_parameter_count():
-    assert R.PARAMS == 55080
+    assert R.PARAMS == 56120
 
 
 def test_backward_matches_finite_differences():
     rng = np.random.default_rng(0)
     p = init(rng)
     x = rng.normal(0, 1, (3, R.FEATURES))
-    y = (rng.random((3, 8)) < 0.5).astype(np.float64)
-    w = np.ones((3, 8))
+    y = (rng.random((3, R.OUTPUTS)) < 0.5).astype(np.float64)
+    w = np.ones((3, R.OUTPUTS))
     z, cache = R.forward(p, x, bf=False)
     _, dz = R.bce(z, y, w)
     g = R.backward(p, cache, dz.astype(np.float64), bf=False)

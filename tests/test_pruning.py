@@ -53,3 +53,50 @@ def test_key_frames_ignore_masks(oracle):
     want = oracle.decide(w, h, src, [], lam.lambda_q8(120))
     got, _ = oracle.decide_masked(w, h, src, [], lam.lambda_q8(120), np.zeros(want.size, np.uint8))
     assert records_equal(got, want)
+
+
+def test_keeping_the_used_options_loses_nothing(oracle):
+    """Masks of exactly the options each superblock's chosen partition uses (references, intra
+    modes, block levels) give every superblock the exhaustive cost."""
+    from celv2_b200.pruner.data import used_options
+
+    for w, h, src, refs in (case(), case(416, 240, 3), case(202, 122, 2)):
+        q = lam.lambda_q8(120)
+        full_rec, full = oracle.decide_masked(w, h, src, refs, q)
+        keep = used_options(full_rec, len(refs))
+        assert (keep & 0xF00).all() and (keep & 0x7F).all()
+        got, cost = oracle.decide_masked(w, h, src, refs, q, keep)
+        assert np.array_equal(cost, full)
+
+
+def test_pruned_levels_and_modes_are_never_chosen(oracle):
+    """Random level and intra-mode masks: the chosen leaves use only kept levels and modes, the
+    records of pruned-level blocks read as blocks with no choice, and no superblock gets cheaper."""
+    from celv2_b200.pruner.data import block_level
+
+    w, h, src, refs = case()
+    nsb = ((w + 63) // 64) * ((h + 63) // 64)
+    rng = np.random.default_rng(11)
+    q = lam.lambda_q8(120)
+    _, full = oracle.decide_masked(w, h, src, refs, q)
+    for trial in range(6):
+        levels = rng.integers(1, 16, nsb).astype(np.uint32)
+        modes = rng.integers(1, 1 << 13, nsb).astype(np.uint32)
+        keep = 0x87 | levels << 8 | modes << 16
+        got, cost = oracle.decide_masked(w, h, src, refs, q, keep)
+        assert (cost >= full).all() and (cost < 1 << 56).all()
+        for i, o in enumerate(got):
+            n = int(o["nblocks"])
+            lv = block_level(o["w4"][:n], o["h4"][:n])
+            assert all(levels[i] >> int(l) & 1 for l in lv), (trial, i)
+            for k in range(n):
+                m = int(o["mode"][k])
+                if m != 13:
+                    assert modes[i] >> m & 1
+            for b in range(425):
+                sq = b // 5
+                level = 3 if sq >= 21 else 2 if sq >= 5 else 1 if sq >= 1 else 0
+                if not levels[i] >> level & 1:
+                    assert o["c_inter_cost"][b] == np.iinfo(np.int64).max
+                    assert o["c_intra_cost"][b] == np.iinfo(np.int64).max
+                    assert (o["c_rcost"][:, b] == NO_REF_COST).all()
