@@ -60,13 +60,31 @@ struct InterSmem {
   int nd[kMaxRegions];
   unsigned char list[kSlots];         // per candidate slot: its MV index in its region's D (255: pruned block)
   unsigned key[kBlocks];              // per block: least (SATD << 7 | candidate index) so far
-  unsigned short tile[kChunk][256];   // 4x4 SATDs (at most 16 x 4 x 255 = 16,320)
-  unsigned short whole8[kChunk][64];  // 8x8 sums (at most 65,280)
-  int sum16[kChunk][16];
 };
 
+// The per-chunk sums follow InterSmem in shared memory, sized by the launch's chunk (a smaller
+// chunk leaves more of the SM's memory to the L1 cache the prediction rows go through).
+struct ChunkSums {
+  unsigned short (*tile)[256];   // [chunk][256] 4x4 SATDs (at most 16 x 4 x 255 = 16,320)
+  unsigned short (*whole8)[64];  // [chunk][64] 8x8 sums (at most 65,280)
+  int (*sum16)[16];              // [chunk][16] 16x16 sums
+};
+
+__host__ __device__ constexpr size_t inter_smem_bytes(int chunk) {
+  return (sizeof(InterSmem) + 15) / 16 * 16 + (size_t)chunk * (256 * 2 + 64 * 2 + 16 * 4);
+}
+
+__device__ __forceinline__ ChunkSums chunk_sums(unsigned char* base, int chunk) {
+  unsigned char* p = base + (sizeof(InterSmem) + 15) / 16 * 16;
+  ChunkSums c;
+  c.tile = reinterpret_cast<unsigned short (*)[256]>(p);
+  c.whole8 = reinterpret_cast<unsigned short (*)[64]>(p + (size_t)chunk * 512);
+  c.sum16 = reinterpret_cast<int (*)[16]>(p + (size_t)chunk * 640);
+  return c;
+}
+
 // SATD of block b at chunk-local MV dd from the shared sums.
-__device__ __forceinline__ int block_satd(const InterSmem& S, int b, int dd) {
+__device__ __forceinline__ int block_satd(const ChunkSums& S, int b, int dd) {
   const int sq = b / 5, kind = b - sq * 5;
   if (sq >= 21) {  // 8x8 cell c: its tiles t, t + 1, t + 16, t + 17
     const int c = sq - 21, t = (c >> 3) * 32 + (c & 7) * 2;
@@ -138,6 +156,7 @@ __host__ __device__ __forceinline__ int candidate_cell(int bx, int by, int bw, i
 __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __restrict__ jobs, WorkList w, int chunk) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   InterSmem& S = *reinterpret_cast<InterSmem*>(smem_raw);
+  const ChunkSums Q = chunk_sums(smem_raw, chunk);
   __shared__ int unit_slot;
   const int tid = threadIdx.x, lane = tid & 31;
   int unit, iter = 0;
@@ -269,16 +288,16 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
         int v = sat[h] + __shfl_xor_sync(0xffffffffu, sat[h], 1);
         v += __shfl_xor_sync(0xffffffffu, v, 16);
         if (dd + h < nc) {
-          S.tile[dd + h][tid] = (unsigned short)sat[h];
-          if (lane < 16 && !(lane & 1)) S.whole8[dd + h][(tid >> 5) * 8 + (lane >> 1)] = (unsigned short)v;
+          Q.tile[dd + h][tid] = (unsigned short)sat[h];
+          if (lane < 16 && !(lane & 1)) Q.whole8[dd + h][(tid >> 5) * 8 + (lane >> 1)] = (unsigned short)v;
         }
       }
     }
     __syncthreads();
     for (int k = tid; k < nc * 16; k += kInterThreads) {
       const int dd = k >> 4, i = k & 15, c = (i >> 2) * 16 + (i & 3) * 2;
-      const unsigned short* W = S.whole8[dd];
-      S.sum16[dd][i] = W[c] + W[c + 1] + W[c + 8] + W[c + 9];
+      const unsigned short* W = Q.whole8[dd];
+      Q.sum16[dd][i] = W[c] + W[c + 1] + W[c + 8] + W[c + 9];
     }
     __syncthreads();
     // 3. every candidate slot whose MV is in this chunk (the slot's region's MVs)
@@ -287,7 +306,7 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
       if (d < 0 || d >= nc) continue;  // 255: a pruned block
       const unsigned bp = g_slot[k];
       const int b = bp & 511, kk = (bp >> 9) & 127;
-      atomicMin(&S.key[b], ((unsigned)block_satd(S, b, d) << 7) | (unsigned)kk);
+      atomicMin(&S.key[b], ((unsigned)block_satd(Q, b, d) << 7) | (unsigned)kk);
     }
     __syncthreads();  // the next chunk overwrites the sums
   }
@@ -307,8 +326,9 @@ void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, cudaStream
   const int units = w.prefix[w.njobs];
   if (units <= 0) return;
   chunk = chunk < 8 ? 8 : chunk > kChunk ? kChunk : chunk;
-  const int grid = w.queue ? persistent_grid((const void*)k_inter, kInterThreads, sizeof(InterSmem), units) : units;
-  k_inter<<<grid, kInterThreads, sizeof(InterSmem), st>>>(jobs, w, chunk);
+  const size_t smem = inter_smem_bytes(chunk);
+  const int grid = w.queue ? persistent_grid((const void*)k_inter, kInterThreads, smem, units) : units;
+  k_inter<<<grid, kInterThreads, smem, st>>>(jobs, w, chunk);
 }
 
 cudaError_t inter_attributes() {
@@ -338,8 +358,7 @@ cudaError_t inter_attributes() {
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_cand_cell, cell, sizeof cell);
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_slot, slot, sizeof slot);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(InterSmem));
-  if (e == cudaSuccess) persistent_grid((const void*)k_inter, kInterThreads, sizeof(InterSmem), 1);  // fills the grid cache
+  e = cudaFuncSetAttribute(k_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inter_smem_bytes(kChunk));
   return e;
 }
 
