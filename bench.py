@@ -556,7 +556,7 @@ def run_batches(engines, batches, qindex, record=None):
             record(k)
 
 
-def run_multi_stream(args, stream_of, dist, local, cpu_1080p_s):
+def run_multi_stream(args, stream_of, dist, local, cpu_1080p_s, rank: int = 0, world: int = 1):
     """Six concurrent streams of uneven size (the multi-stream configuration): 33 frames each in
     16-frame mini-GOPs, refs 7, qindex 130, the sinusoid workload's content at each size. Every
     coding group of all streams is one multi-resolution batch (split into parts of at most 30 jobs),
@@ -565,15 +565,24 @@ def run_multi_stream(args, stream_of, dist, local, cpu_1080p_s):
     size, each size tuned alone, beside it). Reports aggregate superblocks/s and frames/s over the
     timed steps (frames resident in HBM, records left on the device as in `value`), per-stream
     frame latency (the GPU time of the batch that decided the frame: mean and max over the
-    stream's frames), and the reference CpuEngine's seconds per 7-reference frame per size."""
+    stream's frames), and the reference CpuEngine's seconds per 7-reference frame per size. On
+    several GPUs each rank decides whole streams (gop.assign_streams), no data crossing between
+    them, timed as the max over ranks."""
     import torch
 
     from celv2_b200 import engine as E
     from celv2_b200 import gop, synth, tune
 
     plan = gop.stream_plan(C3_FRAMES)
-    clips = [synth.hd_clip(seed=200 + k, frames=C3_FRAMES, width=w, height=h) for k, (w, h) in enumerate(C3_SIZES)]
-    engines = [E.CudaEngine(w, h, device=local) for w, h in C3_SIZES]
+    mine = gop.assign_streams(C3_SIZES, [C3_FRAMES] * len(C3_SIZES), world)[rank]
+    steps = max(1, min(args.steps, 8))
+    if not mine:  # more ranks than streams: this one only joins the timing
+        timed_on(torch.cuda.current_stream(local), lambda: None, steps, dist, local)
+        return None
+    sizes = [C3_SIZES[i] for i in mine]
+    clips = [synth.hd_clip(seed=200 + k, frames=C3_FRAMES, width=C3_SIZES[k][0], height=C3_SIZES[k][1])
+             for k in mine]
+    engines = [E.CudaEngine(w, h, device=local) for w, h in sizes]
     try:
         for e, clip in zip(engines, clips):
             e.reserve_group(8)
@@ -581,7 +590,7 @@ def run_multi_stream(args, stream_of, dist, local, cpu_1080p_s):
                 e.upload(f.hy, i)
         leaf_src, leaf_refs = plan[7][0]  # a 7-reference leaf of the first mini-GOP
         per_size = {}
-        for (w, h), e in zip(C3_SIZES, engines):
+        for (w, h), e in zip(sizes, engines):
             if f"{w}x{h}" not in per_size:
                 ch = tune.autotune(e, leaf_src, leaf_refs, QINDEX, reps=2)
                 per_size[f"{w}x{h}"] = {k: v for k, v in ch.items() if k != "stage_ms"}
@@ -594,7 +603,6 @@ def run_multi_stream(args, stream_of, dist, local, cpu_1080p_s):
             run_batches(engines, batches, QINDEX)
         for e in engines:
             e.finish()
-        steps = max(1, min(args.steps, 8))
         ms = timed_on(stream, lambda: run_batches(engines, batches, QINDEX), steps, dist, local)
         # latencies: an event after every batch of one more step
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(batches) + 1)]
@@ -606,22 +614,23 @@ def run_multi_stream(args, stream_of, dist, local, cpu_1080p_s):
     finally:
         for e in engines:
             e.close()
-    nsb = [((w + 63) // 64) * ((h + 63) // 64) for w, h in C3_SIZES]
-    frames = C3_FRAMES * len(C3_SIZES) * steps
-    sbs = C3_FRAMES * sum(nsb) * steps
+    nsb_all = [((w + 63) // 64) * ((h + 63) // 64) for w, h in C3_SIZES]
+    nsb = [nsb_all[k] for k in mine]
+    frames = C3_FRAMES * len(C3_SIZES) * steps  # every rank's streams
+    sbs = C3_FRAMES * sum(nsb_all) * steps
     streams = []
-    for i, (w, h) in enumerate(C3_SIZES):
-        mine = [lat[k] for k, b in enumerate(batches) for j, _, _ in b if j == i]
+    for i, (w, h) in enumerate(sizes):
+        lats = [lat[k] for k, b in enumerate(batches) for j, _, _ in b if j == i]
         streams.append({"size": f"{w}x{h}", "superblocks": nsb[i], "frames": C3_FRAMES,
-                        "latency_ms_mean": sum(mine) / len(mine), "latency_ms_max": max(mine)})
+                        "latency_ms_mean": sum(lats) / len(lats), "latency_ms_max": max(lats)})
     cpu = {}
-    if not args.no_cpu_baseline:
+    if not args.no_cpu_baseline and world == 1:
         for k, (w, h) in enumerate(C3_SIZES):
             key = f"{w}x{h}"
             if key in cpu:
                 continue
             if w * h > 1920 * 1080:
-                cpu[key] = {"s_per_frame": cpu_1080p_s * nsb[k] / 510 if cpu_1080p_s else None,
+                cpu[key] = {"s_per_frame": cpu_1080p_s * nsb_all[k] / 510 if cpu_1080p_s else None,
                             "how": "the 1080p measurement scaled by superblocks (a 4K frame takes ~50 s)"}
             elif (w, h) == (1920, 1080):
                 cpu[key] = {"s_per_frame": cpu_1080p_s, "how": "measured (cpu_baseline)"}
@@ -631,6 +640,7 @@ def run_multi_stream(args, stream_of, dist, local, cpu_1080p_s):
     return {"workload": "6 streams 640x360, 960x540, 1280x720, 1920x1080 x2, 3840x2160; 33 frames each, "
                         "16-frame mini-GOPs, refs 7, qindex 130; every coding group of all streams as one "
                         "multi-resolution batch (celv2_launch_multi)",
+            "ranks": world, "rank0_streams": mine,
             "superblocks_per_s": sbs / (ms / 1e3), "frames_per_s": frames / (ms / 1e3), "steps": steps,
             "ms_per_step": ms / steps, "batches_per_step": len(batches), "streams": streams,
             "tuned_batch": {k: v for k, v in tuned.items() if k != "stage_ms"}, "tuned_per_size": per_size,
@@ -824,7 +834,7 @@ def run_cuda_arm(args):
         cpu_1080p_s = 1.0 / fps
 
     # the single-GPU configurations of several streams (replicas at N > 1 would only repeat them)
-    multi = run_multi_stream(args, stream_of, None, local, cpu_1080p_s) if world == 1 and not args.no_multi else None
+    multi = None if args.no_multi else run_multi_stream(args, stream_of, dist, local, cpu_1080p_s, rank, world)
     anime = run_anime(args, stream_of, None, local, cpu_1080p_s) if world == 1 and not args.no_anime else None
 
     line = None
@@ -892,8 +902,11 @@ def run_cuda_arm(args):
 
 def run_profile_case(args):
     """The small case for ncu: one 7-reference 1080p leaf decided twice, frames resident in HBM
-    (8 frames with phase planes, about 0.6 GB). Kernel order per decision: k_me_level x5
-    (levels 4..0), k_intra, k_inter, k_finalize."""
+    (8 frames with phase planes, about 0.6 GB), then a third time with every superblock keeping only
+    the 16- and 8-sample block levels (the pruned search's 16x16-region inter path). Kernel order
+    per decision: k_me_level x5 (levels 4..0), k_me_refine, k_intra, k_inter, k_finalize."""
+    import numpy as np
+
     from celv2_b200 import engine as E
 
     clip = make_clip(SEED)[:8]
@@ -902,6 +915,8 @@ def run_profile_case(args):
         eng.upload(f.hy, i)
     for _ in range(2):
         eng.launch_group([7], [[6, 5, 4, 3, 2, 1, 0]], QINDEX)
+    eng.set_keep(0, np.full(eng.sb_cols * eng.sb_rows, 0xFF | 0xC00, np.uint32))
+    eng.launch_group([7], [[6, 5, 4, 3, 2, 1, 0]], QINDEX)
     eng.finish()
     eng.close()
     print("profile case: done")

@@ -81,3 +81,18 @@ def stream_plan(nframes: int, gop: int = 16, refs: int = 7, cuts=()):
                 groups.append([(d, refs_of(d)) for d in leaves])
             lo = anchor
     return groups
+
+
+def assign_streams(sizes, frames, world: int):
+    """Whole streams to GPUs (ranks) for several concurrent streams: stream i (width, height) with
+    frames[i] frames goes to one rank, largest first onto the least loaded rank (work = superblocks
+    x frames; ties to the lower rank). Streams are independent, so no data crosses between GPUs.
+    Returns each rank's stream indices (ascending). Every rank computes the same assignment."""
+    work = [((w + 63) // 64) * ((h + 63) // 64) * f for (w, h), f in zip(sizes, frames)]
+    load = [0] * world
+    out = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda i: (-work[i], i)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        load[r] += work[i]
+        out[r].append(i)
+    return [sorted(o) for o in out]

@@ -116,3 +116,48 @@ def test_two_rank_max_over_ranks_gloo():
     for p in ps:
         p.join(60)
     assert got == [(0, 20.0), (1, 20.0)]
+
+
+def _stream_rank(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+
+    from celv2_b200 import gop
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        sizes = [(3840, 2160), (1920, 1080), (1920, 1080), (1280, 720), (960, 540), (640, 360)]
+        mine = gop.assign_streams(sizes, [33] * 6, world)[rank]
+        sbs = sum(((w + 63) // 64) * ((h + 63) // 64) * 33 for w, h in (sizes[i] for i in mine))
+        t = torch.tensor([sbs], dtype=torch.float64)
+        dist.all_reduce(t)  # the aggregate superblocks of the multi-stream configuration
+        out.put((rank, mine, int(t.item())))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_streams_shard_across_two_ranks_gloo():
+    """Whole streams to ranks (the multi-stream configuration on 2 GPUs): each stream on exactly
+    one rank, the 4K stream alone on one, and the ranks' superblocks sum to the whole workload."""
+    import multiprocessing as mp
+    import socket
+
+    from celv2_b200 import gop
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_stream_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    got = sorted(q.get(timeout=120) for _ in ps)
+    for p in ps:
+        p.join(60)
+    assert sorted(got[0][1] + got[1][1]) == list(range(6))
+    assert got[0][1] == [0] and got[1][1] == [1, 2, 3, 4, 5]  # 2040 x 33 against 2070 x 33 superblocks
+    assert got[0][2] == got[1][2] == 33 * (2040 + 510 + 510 + 240 + 135 + 60)
+    assert gop.assign_streams([(640, 360)] * 3, [33] * 3, 4) == [[0], [1], [2], []]
