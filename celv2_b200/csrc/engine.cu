@@ -270,7 +270,7 @@ struct celv2_engine {
   unsigned* queues = nullptr;
   bool persistent = true;      // the queue-draining persistent stage kernels (else one CTA per unit)
   unsigned persistent_off = 0; // stages (bit i: queue i) that run one CTA per unit anyway
-  int me_cells[kLevels] = {32, 32, 32, 32, 32};
+  int me_cells[kLevels] = {30, 30, 30, 30, 30};
   // the learned pruner: features on request, the network when parameters are set
   bool features_on = false;
   float* pruner_params = nullptr;  // device, CELV2_PRUNER_PARAMS floats
@@ -1464,7 +1464,7 @@ int celv2_set_config(celv2_engine* e, int key, int value) {
       case CELV2_CFG_ME_CELLS_L0 + 2:
       case CELV2_CFG_ME_CELLS_L0 + 3:
       case CELV2_CFG_ME_CELLS_L0 + 4:
-        if (value != 16 && value != 32) invalid("motion-search cells per CTA must be 16 or 32");
+        if (value != 15 && value != 30) invalid("motion-search cells per CTA must be 15 or 30");
         e->me_cells[key - CELV2_CFG_ME_CELLS_L0] = value, e->free_graphs();
         break;
       default: invalid("unknown configuration key");

@@ -5,7 +5,7 @@
 // (:122-133), me_refine (:141-154), me_cell (:162-193); driven level by level, coarsest first,
 // as src/gpu/cpu_engine.cpp:68-83 does.
 //
-// One CTA per 32 consecutive 8x8 cells of one (job, reference):
+// One CTA per 30 (or 15) consecutive 8x8 cells of one (job, reference):
 //  A. the cells' cur blocks are staged in shared memory; one thread per (cell, predictor centre)
 //     computes the six centre SADs;
 //  B. one thread per cell replays the reference's sequential choice of the two best distinct
@@ -27,8 +27,11 @@ constexpr int kMeThreads = 256;
 constexpr int kWinRows = 24, kWinWords = 8;    // a window row: 32 bytes from an 8-byte boundary
 constexpr int kWinStride = kWinRows * kWinWords + 8;  // +8 words: neighbouring windows use other banks
 
-// Shared state of a CTA of CELLS cells (16 or 32: fewer cells per CTA give small pyramid levels
-// more CTAs; the autotuner picks per level).
+// Shared state of a CTA of CELLS cells (15 or 30: fewer cells per CTA give small pyramid levels
+// more CTAs; the autotuner picks per level). Nearly every cell searches two centres, so a CTA's
+// search phase has about 2 x 17 x CELLS (search, column) items: 30 and 15 cells make 1,020 and 510,
+// four and two nearly full rounds of 256 threads (32 and 16 cells left a last round 25% and 12%
+// full).
 template <int CELLS>
 struct MeSmem {
   static constexpr int kSearches = 2 * CELLS;  // at most two centres per cell
@@ -369,10 +372,10 @@ static void launch_cells(const FrameJob* jobs, const WorkList& w, int level, cud
 
 void launch_me_level(const FrameJob* jobs, const WorkList& w, int level, int cells, cudaStream_t st) {
   if (w.prefix[w.njobs] <= 0) return;
-  if (cells == 16)
-    launch_cells<16>(jobs, w, level, st);
+  if (cells == 15)
+    launch_cells<15>(jobs, w, level, st);
   else
-    launch_cells<32>(jobs, w, level, st);
+    launch_cells<30>(jobs, w, level, st);
 }
 
 template <int CELLS>
@@ -384,8 +387,8 @@ static cudaError_t attributes_cells() {
 }
 
 cudaError_t me_attributes() {
-  cudaError_t e = attributes_cells<16>();
-  if (e == cudaSuccess) e = attributes_cells<32>();
+  cudaError_t e = attributes_cells<15>();
+  if (e == cudaSuccess) e = attributes_cells<30>();
   if (e == cudaSuccess) persistent_grid((const void*)k_me_refine, kRefineThreads, 0, 1);  // fills the grid cache
   return e;
 }

@@ -2,7 +2,7 @@
 
 The decisions never depend on these knobs (the tests check every one against the oracle); only the
 speed does. For one resolution it times the stage kernels under every combination of
-  - motion-search cells per CTA (16 or 32),
+  - motion-search cells per CTA (15 or 30),
   - persistent queue-draining grid or one CTA per unit,
   - inter MV chunk (32 or 64),
 on a representative job (a frame and its references already in the engine's store), with the
@@ -43,7 +43,7 @@ def autotune_run(eng: E.CudaEngine, run, reps: int = 3) -> dict:
     run()  # warm-up
     results = []
     try:
-        for cells, persistent, chunk in itertools.product((16, 32), (0, 1), (32, 64)):
+        for cells, persistent, chunk in itertools.product((15, 30), (0, 1), (32, 64)):
             for l in range(5):
                 eng.set_config(E.CFG_ME_CELLS_L0 + l, cells)
             eng.set_config(E.CFG_PERSISTENT_OFF, 0 if persistent else 0x1FF)
@@ -59,7 +59,7 @@ def autotune_run(eng: E.CudaEngine, run, reps: int = 3) -> dict:
     chosen = {"me_cells": [], "persistent_off": 0, "inter_chunk": 64, "stage_ms": {}}
     for l in range(5):
         b = best(f"me_l{l}", None)
-        cells, persistent = (b[0], b[1]) if b else (32, 1)
+        cells, persistent = (b[0], b[1]) if b else (30, 1)
         chosen["me_cells"].append(cells)
         if not persistent:
             chosen["persistent_off"] |= 1 << l

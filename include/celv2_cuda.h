@@ -189,8 +189,8 @@ long long celv2_kernel_launches(const celv2_engine* e);
  *    CELV2_CFG_PERSISTENT is on (bit l: motion-search level l, 5 intra, 6 inter, 7 finalize,
  *    8 level 0's quarter-pel refinement).
  *  CELV2_CFG_INTER_CHUNK: distinct MVs per pass of the inter stage, 8..64 (default 64).
- *  CELV2_CFG_ME_CELLS_L0 + l: 8x8 cells per motion-search CTA at pyramid level l, 16 or 32
- *    (default 32).
+ *  CELV2_CFG_ME_CELLS_L0 + l: 8x8 cells per motion-search CTA at pyramid level l, 15 or 30
+ *    (default 30).
  *  CELV2_CFG_FEATURES: 1 -- every inter frame's learned-pruner features are kept for
  *    celv2_features (include/celv2_pruner.h); 0 (default) -- only when the pruner runs.
  * The autotuner (celv2_b200/tune.py) times these per frame size and sets the fastest. */

@@ -60,7 +60,7 @@ def test_multi_resolution_batch_matches_oracle(oracle):
             e.close()
 
 
-@pytest.mark.parametrize("cells,chunk,off", [(16, 32, 0), (16, 64, 0x1FF), (32, 32, 0x155)])
+@pytest.mark.parametrize("cells,chunk,off", [(15, 32, 0), (15, 64, 0x1FF), (30, 32, 0x155)])
 def test_tuning_knobs_match_oracle(oracle, cells, chunk, off):
     w, h = 416, 240
     clip = synth.small_clip(seed=23, frames=8)
@@ -85,7 +85,7 @@ def test_autotuner_sets_a_valid_config(tmp_path, monkeypatch):
         for i, f in enumerate(clip):
             e.upload(f.hy, i)
         chosen = tune.cached(e, "test-gpu", 7, [6, 5, 4, 3, 2, 1, 0])
-        assert len(chosen["me_cells"]) == 5 and all(c in (16, 32) for c in chosen["me_cells"])
+        assert len(chosen["me_cells"]) == 5 and all(c in (15, 30) for c in chosen["me_cells"])
         assert chosen["inter_chunk"] in (32, 64)
         assert [e.get_config(E.CFG_ME_CELLS_L0 + l) for l in range(5)] == chosen["me_cells"]
         again = tune.cached(e, "test-gpu", 7, [6, 5, 4, 3, 2, 1, 0])  # from the cache file
