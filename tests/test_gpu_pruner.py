@@ -72,7 +72,7 @@ def test_loss_and_adam_match_oracle():
     w = rng.choice([0.0, 1.0, 2.0], (50, E.PRUNER_OUTPUTS)).astype(np.float32)
     lib = E.library()
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    dz, loss = torch.zeros(400, device="cuda"), torch.zeros(1, device="cuda")
+    dz, loss = torch.zeros(50 * E.PRUNER_OUTPUTS, device="cuda"), torch.zeros(1, device="cuda")
     assert lib.celv2_pruner_bce(ptr(dev(z)), ptr(dev(y)), ptr(dev(w)), 50, ptr(dz), ptr(loss), st) == 0
     want_loss, want_dz = R.bce(z, y, w)
     assert abs(loss.item() - want_loss) < 1e-4 * max(1.0, abs(want_loss))
