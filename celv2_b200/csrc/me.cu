@@ -26,6 +26,11 @@ namespace celv2cu {
 constexpr int kMeThreads = 256;
 constexpr int kWinRows = 24, kWinWords = 8;    // a window row: 32 bytes from an 8-byte boundary
 constexpr int kWinStride = kWinRows * kWinWords + 8;  // +8 words: neighbouring windows use other banks
+// A merged search: the two centres of a cell at most 2 apart in x and y searched as one union
+// window of at most 19 x 19 positions (instead of two 17 x 17): 26 rows of 40 bytes, in the space
+// of two windows.
+constexpr int kMergeMax = 2, kUnion = 17 + kMergeMax, kMWinRows = kUnion + 7, kMWinWords = 10;
+static_assert(kMWinRows * kMWinWords <= 2 * kWinStride, "a merged window fits two windows' space");
 
 // Shared state of a CTA of CELLS cells (15 or 30: fewer cells per CTA give small pyramid levels
 // more CTAs; the autotuner picks per level). Nearly every cell searches two centres, so a CTA's
@@ -40,9 +45,12 @@ struct MeSmem {
   int ccx[CELLS][6], ccy[CELLS][6];
   int scell[kSearches], sx[kSearches], sy[kSearches], soff[kSearches];
   unsigned skey[kSearches];
-  int first_search[CELLS], two[CELLS];
+  // merged searches (entries from the back of the list): the second centre and its key
+  int sx2[kSearches], sy2[kSearches];
+  unsigned skey2[kSearches];
+  int first_search[CELLS], two[CELLS];  // two: 0 one centre, 1 two searches, 2 one merged search
   int need[CELLS];  // the cell is searched (level 0 of a pruned job: some superblock reads it)
-  int nsearch;
+  int nsearch, nmerged;
   alignas(16) uint32_t win[kSearches * kWinStride];
 };
 
@@ -94,7 +102,7 @@ __device__ __forceinline__ int sad8(const uint32_t* c, const DevPlane& ref, int 
 __device__ __forceinline__ int refine_pos(int t) { return t == 0 ? 4 : (t <= 4 ? t - 1 : t); }
 
 template <int CELLS>
-__global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restrict__ jobs, WorkList w, int level) {
+__global__ void __launch_bounds__(kMeThreads, 4) k_me_level(const FrameJob* __restrict__ jobs, WorkList w, int level) {
   constexpr int kMeCells = CELLS;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   MeSmem<CELLS>& S = *reinterpret_cast<MeSmem<CELLS>*>(smem_raw);
@@ -121,7 +129,7 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
     const int cell = cell0 + tid, by = cell / cols, bx = cell - by * cols;
     S.need[tid] = tid < ncells && (level != 0 || cell_needed(job, r, bx, by));
   }
-  if (tid == 0) S.nsearch = 0;
+  if (tid == 0) S.nsearch = 0, S.nmerged = 0;
   __syncthreads();
   const bool top = level == kLevels - 1;
   if (!top && tid < kMeCells * 6) {
@@ -161,9 +169,18 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
         }
       }
     }
+    const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
+    if (two && abs(px - px2) <= kMergeMax && abs(py - py2) <= kMergeMax) {
+      // one union window for both centres, its entry from the back of the list
+      const int s = MeSmem<CELLS>::kSearches - 1 - atomicAdd(&S.nmerged, 1);
+      const int ux = min(px, px2) - kMeRange, wx0 = bx * 8 + ux;
+      S.first_search[c] = s, S.two[c] = 2;
+      S.scell[s] = c, S.sx[s] = px, S.sy[s] = py, S.sx2[s] = px2, S.sy2[s] = py2;
+      S.soff[s] = wx0 - (wx0 & ~7);
+      S.skey[s] = S.skey2[s] = 0xffffffffu;
+    } else {
     const int s0 = atomicAdd(&S.nsearch, two ? 2 : 1);
     S.first_search[c] = s0, S.two[c] = two;
-    const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
     for (int k = 0; k < (two ? 2 : 1); k++) {
       const int cxs = k ? px2 : px, cys = k ? py2 : py;
       const int wx0 = bx * 8 + cxs - kMeRange;
@@ -171,9 +188,10 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
       S.soff[s0 + k] = wx0 - (wx0 & ~7);  // the window starts on the 8-byte boundary below wx0
       S.skey[s0 + k] = 0xffffffffu;
     }
+    }
   }
   __syncthreads();
-  const int nsearch = S.nsearch;
+  const int nsearch = S.nsearch, nmerged = S.nmerged;
   // windows: rows y0 + cy - 8 .. + 23, 32 bytes from the 8-byte boundary at or below x0 + cx - 8;
   // inside the margin as asynchronous 8-byte copies (all in flight at once: one memory latency for
   // the whole staging), else word by word with clamping. Plane rows start 8-byte aligned (strides
@@ -185,6 +203,21 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
     const int wx = (bx * 8 + S.sx[s] - kMeRange) & ~7, wy = by * 8 + S.sy[s] - kMeRange;
     uint32_t* dst = S.win + s * kWinStride + rr * kWinWords + 2 * qd;
     if (inside(ref, wx, wy, 4 * kWinWords, kWinRows)) {
+      cp_async8(dst, ref.p + (long long)(wy + rr) * ref.stride + wx + 8 * qd);
+    } else {
+      dst[0] = row4(ref, wx + 8 * qd, wy + rr), dst[1] = row4(ref, wx + 8 * qd + 4, wy + rr);
+    }
+  }
+  // merged windows: rows from min(cy) - 8, 40 bytes from the 8-byte boundary at or below min(cx) - 8;
+  // merged search m (entry kSearches - 1 - m) in the window space of entries kSearches - 2 - 2m, +1
+  for (int e = tid; e < nmerged * kMWinRows * 5; e += kMeThreads) {
+    const int m = e / (kMWinRows * 5), rem = e - m * (kMWinRows * 5);
+    const int rr = rem / 5, qd = rem - rr * 5, s = MeSmem<CELLS>::kSearches - 1 - m;
+    const int cell = cell0 + S.scell[s], by = cell / cols, bx = cell - by * cols;
+    const int wx = (bx * 8 + min(S.sx[s], S.sx2[s]) - kMeRange) & ~7;
+    const int wy = by * 8 + min(S.sy[s], S.sy2[s]) - kMeRange;
+    uint32_t* dst = S.win + (MeSmem<CELLS>::kSearches - 2 - 2 * m) * kWinStride + rr * kMWinWords + 2 * qd;
+    if (inside(ref, wx, wy, 4 * kMWinWords, kMWinRows)) {
       cp_async8(dst, ref.p + (long long)(wy + rr) * ref.stride + wx + 8 * qd);
     } else {
       dst[0] = row4(ref, wx + 8 * qd, wy + rr), dst[1] = row4(ref, wx + 8 * qd + 4, wy + rr);
@@ -226,14 +259,65 @@ __global__ void __launch_bounds__(kMeThreads) k_me_level(const FrameJob* __restr
     }
     atomicMin(&S.skey[s], best);
   }
+  // merged searches: a thread per union column (at most 19); every union position's SAD is the
+  // same for both centres, and each centre takes its own penalty and raster index -- the same keys
+  // as its own 17 x 17 search, so the same first strict minimum
+  for (int item = tid; item < nmerged * kUnion; item += kMeThreads) {
+    const int m = item / kUnion, du = item - m * kUnion, s = MeSmem<CELLS>::kSearches - 1 - m;
+    const int cx1 = S.sx[s], cy1 = S.sy[s], cx2 = S.sx2[s], cy2 = S.sy2[s];
+    const int ux = min(cx1, cx2), uy = min(cy1, cy2);  // union position 0 = centre offset -8
+    if (du >= 17 + abs(cx1 - cx2)) continue;
+    const int nrow = 17 + abs(cy1 - cy2);
+    const uint32_t* c = S.cur[S.scell[s]];
+    uint32_t cw[16];
+#pragma unroll
+    for (int k = 0; k < 16; k++) cw[k] = c[k];
+    const int b = S.soff[s] + du, wi = b >> 2;
+    const unsigned sh = (unsigned)(b & 3) * 8;
+    const uint32_t* wr = S.win + (MeSmem<CELLS>::kSearches - 2 - 2 * m) * kWinStride + wi;
+    unsigned acc[kUnion];
+#pragma unroll
+    for (int k = 0; k < kUnion; k++) acc[k] = 0;
+#pragma unroll
+    for (int rr = 0; rr < kMWinRows; rr++) {
+      const uint32_t u0 = wr[rr * kMWinWords], u1 = wr[rr * kMWinWords + 1], u2 = wr[rr * kMWinWords + 2];
+      const uint32_t w0 = __funnelshift_r(u0, u1, sh), w1 = __funnelshift_r(u1, u2, sh);
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const int dy = rr - i;
+        if (dy >= 0 && dy < kUnion && dy < nrow)
+          acc[dy] = sad4_acc(cw[2 * i + 1], w1, sad4_acc(cw[2 * i], w0, acc[dy]));
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      // union column du is the offset ux - 8 + du, column ux + du - c of the window around centre c
+      const int dx = ux + du - (t ? cx2 : cx1);  // column in this centre's 17 x 17 window
+      const int oy = uy - (t ? cy2 : cy1);       // union row 0's row in its window
+      if (dx < 0 || dx > 16) continue;
+      unsigned best = 0xffffffffu;
+      const unsigned pen_x = kMePenalty * abs(dx - kMeRange);
+#pragma unroll
+      for (int du_y = 0; du_y < kUnion; du_y++) {
+        const int dy = oy + du_y;
+        if (du_y >= nrow || dy < 0 || dy > 16) continue;
+        const unsigned cost = acc[du_y] + pen_x + kMePenalty * abs(dy - kMeRange);
+        const unsigned key = (cost << 9) | (unsigned)(dy * 17 + dx);
+        best = key < best ? key : best;
+      }
+      atomicMin(t ? &S.skey2[s] : &S.skey[s], best);
+    }
+  }
   __syncthreads();
   if (tid < ncells && S.need[tid]) {
     const int s0 = S.first_search[tid];
     const unsigned k1 = S.skey[s0];
     int mx = S.sx[s0] + (int)(k1 & 511) % 17 - kMeRange, my = S.sy[s0] + (int)(k1 & 511) / 17 - kMeRange;
     if (S.two[tid]) {  // the second centre's result only if strictly cheaper (me_cell, :189-192)
-      const unsigned k2 = S.skey[s0 + 1];
-      if ((k2 >> 9) < (k1 >> 9)) mx = S.sx[s0 + 1] + (int)(k2 & 511) % 17 - kMeRange, my = S.sy[s0 + 1] + (int)(k2 & 511) / 17 - kMeRange;
+      const bool merged = S.two[tid] == 2;
+      const unsigned k2 = merged ? S.skey2[s0] : S.skey[s0 + 1];
+      const int sx2 = merged ? S.sx2[s0] : S.sx[s0 + 1], sy2 = merged ? S.sy2[s0] : S.sy[s0 + 1];
+      if ((k2 >> 9) < (k1 >> 9)) mx = sx2 + (int)(k2 & 511) % 17 - kMeRange, my = sy2 + (int)(k2 & 511) / 17 - kMeRange;
     }
     // level 0 in quarter pels: k_me_refine refines it in place
     job.field[r][level][cell0 + tid] = level == 0 ? pack_mv(mx * 4, my * 4) : pack_mv(mx, my);
