@@ -382,7 +382,8 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob*
     wx0[tid] = (bx * 8 + (mv_x(m) >> 2) - 1) & ~7;
     wy0[tid] = by * 8 + (mv_y(m) >> 2) - 1;
   }
-  __syncthreads();
+  // a unit none of whose cells a kept reference reads (pruned search): nothing to refine
+  if (!__syncthreads_or(tid < ncells && need[tid])) continue;
   // 1. the windows: (phase, row, half) outer, cell inner (lane order); inside the stored plane as
   //    asynchronous 8-byte copies (all in flight at once), else word by word with clamping
   for (int e = tid; e < ncells * kPhases * kRwRows * 2; e += kRefineThreads) {
