@@ -31,9 +31,11 @@ def block_level(w4: np.ndarray, h4: np.ndarray) -> np.ndarray:
 def used_options(records: np.ndarray, nrefs: int) -> np.ndarray:
     """Per superblock the keep word (include/celv2_decision.h) of exactly the options its chosen
     partition uses: the references of its inter leaves (a compound's second too), intra and the
-    modes of its intra leaves, the levels of its leaves. These masks keep the chosen partition
-    available at its cost and remove only options it does not use, so the pruned search finds the
-    same cost (the partition choice is a minimum over a subset that still holds the optimum)."""
+    modes of its intra leaves, the levels of its leaves. These masks keep every block of the chosen
+    partition with its choice at its cost (a block's best reference stays the best of the kept
+    ones, a used compound's two references stay its best two), so the pruned search's cost is at
+    most the exhaustive one -- lower where pruning a reference lets a block try its compound with
+    another second reference, which the exhaustive search never tries."""
     nsb = records.size
     mode = records["mode"].astype(np.int64)
     leaf = np.arange(mode.shape[1])[None, :] < records["nblocks"].astype(np.int64)[:, None]

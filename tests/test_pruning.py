@@ -1,5 +1,8 @@
 """The pruned search's semantics on the oracle (CPU): masks that keep everything change nothing,
-a pruned option is never chosen, and pruning never lowers a superblock's cost."""
+a pruned option is never chosen, and keeping the options the exhaustive partition uses never raises
+a superblock's cost. (Pruning is not monotone in general: the exhaustive search tries a block's
+compound only with its second-best reference, so pruning another reference can make a compound
+with a different second reference available, which may be cheaper.)"""
 import numpy as np
 
 import frames as F
@@ -32,7 +35,6 @@ def test_pruned_options_are_never_chosen(oracle):
     keep = rng.integers(0, 256, nsb).astype(np.uint8)
     _, full = oracle.decide_masked(w, h, src, refs, lam.lambda_q8(120))
     got, cost = oracle.decide_masked(w, h, src, refs, lam.lambda_q8(120), keep)
-    assert (cost >= full).all()  # a subset of the options: never cheaper
     for i, o in enumerate(got):
         k = int(keep[i])
         refs_kept = (k & 7) or 7
@@ -57,7 +59,7 @@ def test_key_frames_ignore_masks(oracle):
 
 def test_keeping_the_used_options_loses_nothing(oracle):
     """Masks of exactly the options each superblock's chosen partition uses (references, intra
-    modes, block levels) give every superblock the exhaustive cost."""
+    modes, block levels) never raise a superblock's cost above the exhaustive one."""
     from celv2_b200.pruner.data import used_options
 
     for w, h, src, refs in (case(), case(416, 240, 3), case(202, 122, 2)):
@@ -66,7 +68,7 @@ def test_keeping_the_used_options_loses_nothing(oracle):
         keep = used_options(full_rec, len(refs))
         assert (keep & 0xF00).all() and (keep & 0x7F).all()
         got, cost = oracle.decide_masked(w, h, src, refs, q, keep)
-        assert np.array_equal(cost, full)
+        assert (cost <= full).all()
 
 
 def test_pruned_levels_and_modes_are_never_chosen(oracle):
@@ -84,7 +86,7 @@ def test_pruned_levels_and_modes_are_never_chosen(oracle):
         modes = rng.integers(1, 1 << 13, nsb).astype(np.uint32)
         keep = 0x87 | levels << 8 | modes << 16
         got, cost = oracle.decide_masked(w, h, src, refs, q, keep)
-        assert (cost >= full).all() and (cost < 1 << 56).all()
+        assert (cost < 1 << 56).all()  # a complete partition of kept blocks
         for i, o in enumerate(got):
             n = int(o["nblocks"])
             lv = block_level(o["w4"][:n], o["h4"][:n])
