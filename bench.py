@@ -824,7 +824,7 @@ def run_cuda_arm(args):
 
     # e2e: host 10-bit planes in, decision records back in host memory, every step
     eng.clear_store()  # the resident frames: the end-to-end steps upload their own
-    e2e = run_e2e(eng, clips, plan, max(1, args.steps), dist, local, world)
+    e2e = None if args.no_e2e else run_e2e(eng, clips, plan, max(1, args.steps), dist, local, world)
     eng.close()
 
     cpu, cpu_1080p_s = None, None
@@ -933,6 +933,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="default launch configuration")
     ap.add_argument("--no-graphs", action="store_true", help="stage-by-stage launches instead of CUDA graphs")
     ap.add_argument("--no-multi", action="store_true", help="skip the six-stream multi-resolution block")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end timing (launch lists under ncu)")
     ap.add_argument("--no-anime", action="store_true", help="skip the 4K animation-like streams block")
     ap.add_argument("--profile", action="store_true", help="the small case for ncu captures")
     args = ap.parse_args()
