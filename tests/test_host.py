@@ -161,3 +161,42 @@ def test_streams_shard_across_two_ranks_gloo():
     assert got[0][1] == [0] and got[1][1] == [1, 2, 3, 4, 5]  # 2040 x 33 against 2070 x 33 superblocks
     assert got[0][2] == got[1][2] == 33 * (2040 + 510 + 510 + 240 + 135 + 60)
     assert gop.assign_streams([(640, 360)] * 3, [33] * 3, 4) == [[0], [1], [2], []]
+
+
+def test_stream_plan_chains_mini_gops_and_cuts():
+    """gop.stream_plan: 17 frames are the mini-GOP plan; 33 frames two mini-GOPs whose second takes
+    its references from an 8-slot buffer (at most 7, nearest display distance first); a scene cut
+    starts over with a KEY frame and no reference from before it."""
+    from celv2_b200 import gop
+
+    assert gop.stream_plan(17) == gop.mini_gop_plan(17)
+    plan = gop.stream_plan(33)
+    frames = [s for g in plan for s, _ in g]
+    assert sorted(frames) == list(range(33))
+    coded = []
+    for g in plan:
+        for s, refs in g:
+            assert len(refs) <= 7 and all(r in coded for r in refs)
+            assert refs == sorted(refs, key=lambda r: (abs(r - s), r))
+        coded += [s for s, _ in g]
+    assert [len(g) for g in plan].count(10) == 2  # two leaf groups
+    cut = gop.stream_plan(65, cuts=[33])
+    assert sorted(s for g in cut for s, _ in g) == list(range(65))
+    for g in cut:
+        for s, refs in g:
+            assert all((r >= 33) == (s >= 33) for r in refs)
+    assert (33, []) in [x for g in cut for x in g]
+
+
+def test_animation_generator():
+    """The animation-like content: flat colours (few distinct values), the scene cut a new picture,
+    deterministic per seed."""
+    from celv2_b200 import synth
+
+    clip = synth.animation_clip(320, 192, 6, seed=4, scene_cut=3)
+    again = synth.animation_clip(320, 192, 6, seed=4, scene_cut=3)
+    assert all(np.array_equal(a.hy, b.hy) for a, b in zip(clip, again))
+    assert len(np.unique(clip[1].y)) < 64
+    step = np.abs(clip[2].y.astype(int) - clip[1].y).mean()
+    cut = np.abs(clip[3].y.astype(int) - clip[2].y).mean()
+    assert cut > step
