@@ -266,7 +266,8 @@ struct celv2_engine {
   long long stage_n[kStages] = {};
   unsigned long long* stats = nullptr;  // device work counters (kStats), while timing
   // stage work queues (device counters): [0..4] motion search levels, [5] intra, [6] inter,
-  // [7] finalize, [8] level 0's refinement of the main stream; [15] prepare's intra
+  // [7] finalize, [8] level 0's refinement, [9] inter by regions, of the main stream; [15]
+  // prepare's intra
   unsigned* queues = nullptr;
   bool persistent = true;      // the queue-draining persistent stage kernels (else one CTA per unit)
   unsigned persistent_off = 0; // stages (bit i: queue i) that run one CTA per unit anyway
@@ -591,7 +592,7 @@ struct celv2_engine {
                      const std::vector<NetJob>& nets) {
     const int n = (int)jobs.size();
     int launched = 0;
-    if (persistent) CK(cudaMemsetAsync(queues, 0, 9 * sizeof(unsigned), stream));
+    if (persistent) CK(cudaMemsetAsync(queues, 0, 10 * sizeof(unsigned), stream));
     auto q = [&](int i) { return persistent && !(persistent_off >> i & 1) ? queues + i : nullptr; };
     WorkList w{};
     w.njobs = n;
@@ -622,7 +623,9 @@ struct celv2_engine {
     for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].nrefs * jobs[j].sb_cols * jobs[j].sb_rows;
     w.queue = q(6);
     if (w.prefix[n] > 0) {
-      stage(kStInter, stream, [&] { launch_inter(djobs, w, inter_chunk, stream); });
+      bool any_keep = false;
+      for (const FrameJob& jb : jobs) any_keep |= jb.keep != nullptr;
+      stage(kStInter, stream, [&] { launch_inter(djobs, w, inter_chunk, any_keep, q(9), stream); });
       launched++;
     }
     for (int j = 0; j < n; j++) w.prefix[j + 1] = w.prefix[j] + jobs[j].sb_cols * jobs[j].sb_rows;

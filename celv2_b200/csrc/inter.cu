@@ -21,11 +21,12 @@
 //     first strict minimum over the candidates in order: a repeated MV (which the reference skips)
 //     has the same SATD as its first occurrence and a larger index, so it never wins.
 // 256 |D| Hadamards per (superblock, reference) instead of up to 68,352 for the blocks one by one.
-// Pruned search: where the superblock keeps no 64-level blocks (no 64x64, 64x32, 32x64), each of
-// its 32x32 regions (16x16 with no 32-level blocks either) is scored on its own: a kept block and
-// all its candidates' cells lie inside its region and the ring of cells around it, so the region's
-// tiles are scored at the distinct MVs of its 6 x 6 (4 x 4) cells only -- exactly the SATDs the
-// whole-superblock pass gives them.
+// Pruned search: where the superblock keeps no 64-level blocks (no 64x64, 64x32, 32x64), a second
+// kernel (k_inter_regions) scores each of its 32x32 regions (16x16 with no 32-level blocks either)
+// on its own: a kept block and all its candidates' cells lie inside its region and the ring of
+// cells around it, so the region's tiles are scored at the distinct MVs of its 6 x 6 (4 x 4) cells
+// only -- exactly the SATDs the whole-superblock pass gives them. The whole-superblock kernel
+// (k_inter) keeps its own code and registers: the units of the two kinds go to the two kernels.
 // The result per (block, reference) is the winning SATD and MV; the lambda terms are added by the
 // finalize stage, which alone needs the costs.
 #include <algorithm>
@@ -50,7 +51,8 @@ __device__ unsigned char g_cand_cell[kSlots];
 constexpr int kMaxRegions = 16;  // 16x16 regions of a superblock
 constexpr int kRegCells = 256;   // regions x neighbourhood cells at most (16 x 16, 4 x 36, 1 x 100)
 
-struct InterSmem {
+// The region pass's shared state.
+struct RegionSmem {
   int nb[kNb];                 // packed MV of each neighbourhood cell
   int D[kRegCells];            // per region r: its distinct MVs at D[r * ncell ..], first occurrence order
   int moff[kRegCells];         // per (region, MV): the superblock's prediction, bytes from the reference's level 0
@@ -62,7 +64,7 @@ struct InterSmem {
   unsigned key[kBlocks];              // per block: least (SATD << 7 | candidate index) so far
 };
 
-// The per-chunk sums follow InterSmem in shared memory, sized by the launch's chunk (a smaller
+// The per-chunk sums follow RegionSmem in shared memory, sized by the launch's chunk (a smaller
 // chunk leaves more of the SM's memory to the L1 cache the prediction rows go through).
 struct ChunkSums {
   unsigned short (*tile)[256];   // [chunk][256] 4x4 SATDs (at most 16 x 4 x 255 = 16,320)
@@ -71,11 +73,11 @@ struct ChunkSums {
 };
 
 __host__ __device__ constexpr size_t inter_smem_bytes(int chunk) {
-  return (sizeof(InterSmem) + 15) / 16 * 16 + (size_t)chunk * (256 * 2 + 64 * 2 + 16 * 4);
+  return (sizeof(RegionSmem) + 15) / 16 * 16 + (size_t)chunk * (256 * 2 + 64 * 2 + 16 * 4);
 }
 
 __device__ __forceinline__ ChunkSums chunk_sums(unsigned char* base, int chunk) {
-  unsigned char* p = base + (sizeof(InterSmem) + 15) / 16 * 16;
+  unsigned char* p = base + (sizeof(RegionSmem) + 15) / 16 * 16;
   ChunkSums c;
   c.tile = reinterpret_cast<unsigned short (*)[256]>(p);
   c.whole8 = reinterpret_cast<unsigned short (*)[64]>(p + (size_t)chunk * 512);
@@ -83,8 +85,25 @@ __device__ __forceinline__ ChunkSums chunk_sums(unsigned char* base, int chunk) 
   return c;
 }
 
-// SATD of block b at chunk-local MV dd from the shared sums.
-__device__ __forceinline__ int block_satd(const ChunkSums& S, int b, int dd) {
+// The whole-superblock pass's shared state (every kept level, the 64-level blocks among them).
+struct WholeSmem {
+  int nb[kNb];  // packed MV of each neighbourhood cell
+  int D[kNb];   // distinct MVs, first occurrence order
+  int first_idx[kNb];
+  unsigned char dmap[kNb];
+  int moff[kNb];  // per MV of D: the superblock's prediction, bytes from the reference's level 0
+  unsigned char mfast[kNb];           // per MV of D: its 64 x 64 prediction lies inside the margin
+  unsigned char list[kSlots];         // per candidate slot: its MV index in D
+  unsigned key[kBlocks];              // per block: least (SATD << 7 | candidate index) so far
+  unsigned short tile[kChunk][256];   // 4x4 SATDs (at most 16 x 4 x 255 = 16,320)
+  unsigned short whole8[kChunk][64];  // 8x8 sums (at most 65,280)
+  int sum16[kChunk][16];
+  int nd;
+};
+
+// SATD of block b at chunk-local MV dd from the shared sums (WholeSmem or ChunkSums).
+template <typename Sums>
+__device__ __forceinline__ int block_satd(const Sums& S, int b, int dd) {
   const int sq = b / 5, kind = b - sq * 5;
   if (sq >= 21) {  // 8x8 cell c: its tiles t, t + 1, t + 16, t + 17
     const int c = sq - 21, t = (c >> 3) * 32 + (c & 7) * 2;
@@ -155,7 +174,151 @@ __host__ __device__ __forceinline__ int candidate_cell(int bx, int by, int bw, i
 
 __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __restrict__ jobs, WorkList w, int chunk) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  InterSmem& S = *reinterpret_cast<InterSmem*>(smem_raw);
+  WholeSmem& S = *reinterpret_cast<WholeSmem*>(smem_raw);
+  __shared__ int warp_cnt[kInterThreads / 32];
+  __shared__ int unit_slot;
+  const int tid = threadIdx.x, lane = tid & 31;
+  int unit, iter = 0;
+  while (take_unit(w, unit, iter, &unit_slot)) {
+  const int jb = job_of(w, unit);
+  const FrameJob& job = jobs[jb];
+  const int nsb = job.sb_cols * job.sb_rows;
+  const int u = unit - w.prefix[jb];
+  const int r = u / nsb, sb = u - r * nsb, sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
+  const unsigned keep = keep_mask(job, sb);
+  // a pruned (superblock, reference) is not scored; without 64-level blocks k_inter_regions scores it
+  if (!(keep >> r & 1u) || !(keep & CELV2_KEEP_LEVEL(0))) continue;
+  const int ox = sbx * 64, oy = sby * 64;
+  const int cols = job.fcols[0], rows = job.frows[0];
+  const int* field = job.field[r][0];
+
+  // 1. neighbourhood MVs, their distinct set (first occurrence order), the blocks' lists
+  if (tid < kNb) {
+    const int ny = tid / 10, nx = tid - ny * 10;
+    const int cx = clampi(sbx * 8 - 1 + nx, 0, cols - 1), cy = clampi(sby * 8 - 1 + ny, 0, rows - 1);
+    S.nb[tid] = field[cy * cols + cx];
+  }
+  for (int b = tid; b < kBlocks; b += kInterThreads) S.key[b] = 0xffffffffu;
+  __syncthreads();
+  bool is_first = false;
+  int firstj = 0;
+  if (tid < kNb) {
+    const int v = S.nb[tid];
+    while (S.nb[firstj] != v) firstj++;
+    is_first = firstj == tid;
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, is_first);
+  if (lane == 0) warp_cnt[tid >> 5] = __popc(bal);
+  __syncthreads();
+  if (tid < kNb) {
+    int pos = __popc(bal & ((1u << lane) - 1u));
+    for (int k = 0; k < (tid >> 5); k++) pos += warp_cnt[k];
+    if (is_first) S.D[pos] = S.nb[tid], S.first_idx[tid] = pos;
+  }
+  if (tid == 0) S.nd = warp_cnt[0] + warp_cnt[1] + warp_cnt[2] + warp_cnt[3];
+  __syncthreads();
+  if (tid < kNb) S.dmap[tid] = (unsigned char)S.first_idx[firstj];
+  const int nd = S.nd;
+  if (tid == 0 && job.stats) atomicAdd(job.stats + kStatInterMvs, (unsigned long long)nd * 256);
+  const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
+  if (tid < nd) {
+    const int m = S.D[tid], mx = mv_x(m), my = mv_y(m), x = ox + (mx >> 2), y = oy + (my >> 2);
+    const long long o = (long long)((my & 3) * 4 + (mx & 3)) * ref.phase + (long long)y * ref.stride + x;
+    S.moff[tid] = (int)o;
+    S.mfast[tid] = inside(ref, x, y, 64, 64) && o == (long long)(int)o;
+  }
+  __syncthreads();
+  for (int e = tid; e < kSlots; e += kInterThreads) S.list[e] = S.dmap[g_slot[e] >> 16];
+
+  // this thread's tile: its cur rows, row-transformed, in registers (the grid lies inside the margin)
+  const int tx = tid & 15, ty = tid >> 4;
+  int C[16];
+  {
+    uint32_t c[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) c[i] = load4(cur.p + (long long)(oy + ty * 4 + i) * cur.stride + ox + tx * 4);
+    wh_rows_cur(c, C);
+  }
+  // the tile's prediction rows at MV d start at tile_base + moff[d]; words a row apart are ws apart
+  const uintptr_t tile_base = reinterpret_cast<uintptr_t>(ref.p) + (uintptr_t)(ty * 4 * ref.stride + tx * 4);
+  const int ws = ref.stride >> 2;  // strides are multiples of 64
+  // chunks of equal size, at most `chunk` MVs each
+  const int nchunks = (nd + chunk - 1) / chunk, csize = (nd + nchunks - 1) / nchunks;
+  __syncthreads();  // lists complete
+
+  for (int c0 = 0; c0 < nd; c0 += csize) {
+    const int nc = min(csize, nd - c0);
+    // 2. tile SATDs at every MV of the chunk (two MVs per step for load parallelism); an 8x8
+    //    cell's tiles are lanes l, l + 1, l + 16, l + 17 of one warp
+    for (int dd = 0; dd < nc; dd += 2) {
+      int sat[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int d = c0 + min(dd + h, nc - 1);
+        uint32_t pr[4];
+        if (S.mfast[d]) {  // the usual case, uniform over the CTA: rows from aligned words
+          const uintptr_t a = tile_base + (uintptr_t)(intptr_t)S.moff[d];
+          const uint32_t* wp = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+          const uint32_t sh = (uint32_t)(a & 3) * 8;
+          if (sh == 0) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) pr[i] = __ldg(wp + i * ws);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 4; i++) pr[i] = __funnelshift_r(__ldg(wp + i * ws), __ldg(wp + i * ws + 1), sh);
+          }
+        } else {
+          const int m = S.D[d], mx = mv_x(m), my = mv_y(m);
+          DevPlane ph = ref;
+          ph.p = ref.p + (long long)((my & 3) * 4 + (mx & 3)) * ref.phase;
+          const int x = ox + tx * 4 + (mx >> 2), y = oy + ty * 4 + (my >> 2);
+#pragma unroll
+          for (int i = 0; i < 4; i++) {
+            pr[i] = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) pr[i] |= (uint32_t)at(ph, y + i, x + k) << (8 * k);
+          }
+        }
+        sat[h] = satd4_rows(C, pr);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        int v = sat[h] + __shfl_xor_sync(0xffffffffu, sat[h], 1);
+        v += __shfl_xor_sync(0xffffffffu, v, 16);
+        if (dd + h < nc) {
+          S.tile[dd + h][tid] = (unsigned short)sat[h];
+          if (lane < 16 && !(lane & 1)) S.whole8[dd + h][(tid >> 5) * 8 + (lane >> 1)] = (unsigned short)v;
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < nc * 16; e += kInterThreads) {
+      const int dd = e >> 4, i = e & 15, c = (i >> 2) * 16 + (i & 3) * 2;
+      const unsigned short* W = S.whole8[dd];
+      S.sum16[dd][i] = W[c] + W[c + 1] + W[c + 8] + W[c + 9];
+    }
+    __syncthreads();
+    // 3. every candidate slot whose MV is in this chunk
+    for (int e = tid; e < kSlots; e += kInterThreads) {
+      const int d = (int)S.list[e] - c0;
+      if (d < 0 || d >= nc) continue;
+      const unsigned bp = g_slot[e];
+      const int b = bp & 511, k = (bp >> 9) & 127;
+      atomicMin(&S.key[b], ((unsigned)block_satd(S, b, d) << 7) | (unsigned)k);
+    }
+    __syncthreads();  // the next chunk overwrites the sums
+  }
+  int2* out = job.inter + ((long long)sb * kMaxRefs + r) * kBlocks;
+  for (int b = tid; b < kBlocks; b += kInterThreads) {
+    const unsigned k = S.key[b];
+    out[b] = make_int2((int)(k >> 7), S.D[S.dmap[g_cand_cell[c_cand_off[b] + (k & 127)]]]);
+  }
+  }  // units
+}
+
+__global__ void __launch_bounds__(kInterThreads, 4) k_inter_regions(const FrameJob* __restrict__ jobs, WorkList w, int chunk) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RegionSmem& S = *reinterpret_cast<RegionSmem*>(smem_raw);
   const ChunkSums Q = chunk_sums(smem_raw, chunk);
   __shared__ int unit_slot;
   const int tid = threadIdx.x, lane = tid & 31;
@@ -167,12 +330,13 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   const int u = unit - w.prefix[jb];
   const int r = u / nsb, sb = u - r * nsb, sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
   const unsigned keep = keep_mask(job, sb);
-  if (!(keep >> r & 1u)) continue;  // a pruned (superblock, reference): not scored
+  // a pruned (superblock, reference) is not scored; with 64-level blocks k_inter scores it
+  if (!(keep >> r & 1u) || (keep & CELV2_KEEP_LEVEL(0))) continue;
   const int ox = sbx * 64, oy = sby * 64;
   const int cols = job.fcols[0], rows = job.frows[0];
   const int* field = job.field[r][0];
-  // regions: the whole superblock, or its 32x32 / 16x16 squares where larger blocks are pruned
-  const int R = (keep & CELV2_KEEP_LEVEL(0)) ? 64 : (keep & CELV2_KEEP_LEVEL(1)) ? 32 : 16;
+  // regions: its 32x32 squares, or 16x16 ones where the 32-level blocks are pruned too
+  const int R = (keep & CELV2_KEEP_LEVEL(1)) ? 32 : 16;
   const int nr = 64 / R, nreg = nr * nr, rc = R / 8 + 2, ncell = rc * rc;
 
   // 1. neighbourhood MVs; per region the distinct MVs of its cells (first occurrence order) and
@@ -322,13 +486,19 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   }  // units
 }
 
-void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, cudaStream_t st) {
+void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, bool regions, unsigned* region_queue,
+                  cudaStream_t st) {
   const int units = w.prefix[w.njobs];
   if (units <= 0) return;
   chunk = chunk < 8 ? 8 : chunk > kChunk ? kChunk : chunk;
+  const int grid = w.queue ? persistent_grid((const void*)k_inter, kInterThreads, sizeof(WholeSmem), units) : units;
+  k_inter<<<grid, kInterThreads, sizeof(WholeSmem), st>>>(jobs, w, chunk);
+  if (!regions) return;  // no job has keep words: every unit keeps its 64-level blocks
+  WorkList wr = w;
+  wr.queue = w.queue ? region_queue : nullptr;
   const size_t smem = inter_smem_bytes(chunk);
-  const int grid = w.queue ? persistent_grid((const void*)k_inter, kInterThreads, smem, units) : units;
-  k_inter<<<grid, kInterThreads, smem, st>>>(jobs, w, chunk);
+  const int rgrid = wr.queue ? persistent_grid((const void*)k_inter_regions, kInterThreads, smem, units) : units;
+  k_inter_regions<<<rgrid, kInterThreads, smem, st>>>(jobs, wr, chunk);
 }
 
 cudaError_t inter_attributes() {
@@ -358,7 +528,10 @@ cudaError_t inter_attributes() {
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_cand_cell, cell, sizeof cell);
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_slot, slot, sizeof slot);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inter_smem_bytes(kChunk));
+  e = cudaFuncSetAttribute(k_inter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WholeSmem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_inter_regions, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inter_smem_bytes(kChunk));
+  if (e == cudaSuccess) persistent_grid((const void*)k_inter, kInterThreads, sizeof(WholeSmem), 1);  // fills the grid cache
   return e;
 }
 

@@ -66,8 +66,11 @@ void launch_me_refine(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
 void launch_intra(const FrameJob* jobs, const WorkList& w, cudaStream_t st);
 
 // Each reference's best candidate MV per candidate block, the distinct MVs of a superblock taken
-// in chunks of at most `chunk` (<= 64). Units: nrefs * sb_cols * sb_rows per job.
-void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, cudaStream_t st);
+// in chunks of at most `chunk` (<= 64). Units: nrefs * sb_cols * sb_rows per job. Units that keep
+// their 64-level blocks are scored whole (k_inter); with `regions` (some job has keep words) a
+// second kernel scores the others region by region, draining `region_queue` (zero beforehand).
+void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, bool regions, unsigned* region_queue,
+                  cudaStream_t st);
 
 // Per-block choice, compound, partition choice and the decision records. Units: superblocks.
 void launch_finalize(const FrameJob* jobs, const WorkList& w, cudaStream_t st);

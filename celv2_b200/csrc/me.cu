@@ -16,8 +16,8 @@
 //     one of the 17 dy accumulators whose 8x8 block covers that row -- 24 row loads instead of
 //     17 x 8 per column. The column's best (cost << 9 | raster index) goes to a shared atomicMin,
 //     which yields the reference's first strict minimum in dy-major order;
-// Level 0's quarter-pel refinement is its own kernel (k_me_refine): its phase-plane windows staged in
-// shared memory, one thread per (cell, position, tile) of each step.
+// Level 0's quarter-pel refinement is its own kernel (k_me_refine): a warp per position of a step,
+// a lane per cell.
 // Integer ALU bound: 289 x 16 byte-SIMD absolute-difference accumulates per searched centre.
 #include "kernels.h"
 
@@ -330,32 +330,22 @@ __global__ void __launch_bounds__(kMeThreads, 4) k_me_level(const FrameJob* __re
 }
 
 // ---- quarter-pel refinement of level 0 (me_refine, inter_common.h:141-154) ----
-// One CTA per kRefineCells cells of one (job, reference).
-//  1. The level-0 search leaves whole-pel MVs (multiples of 4 quarter pels), and both steps stay
-//     within 3 quarter pels of them: every position the two steps visit reads its 8x8 block from
-//     rows iy - 1 .. iy + 7 and columns ix - 1 .. ix + 7 of one of the 16 phase planes ((ix, iy)
-//     the block's whole-pel position). So each cell's 9-row window of every phase plane -- 16 bytes
-//     from the 8-byte boundary at or below column ix - 1 -- is staged in shared memory first, by
-//     8-byte cp.async copies that consecutive lanes take for consecutive cells (neighbouring cells
-//     with equal MVs read neighbouring bytes of the same lines).
-//  2. Each step's 9 positions x 4 tiles are (cell, position, tile) items: one 4x4 quarter-pel SATD
-//     each, the prediction rows read from the staged windows (two words and a funnel shift), the
-//     cur tiles row-transformed once per cell; a position's four tiles sit in adjacent lanes and
-//     sum by shuffles; one thread per cell replays the centre-first strict choice.
-constexpr int kRefineCells = 7, kRefineThreads = 256;  // 7 x 36 = 252 items
-constexpr int kRwRows = 9;    // window rows
-constexpr int kRwStride = 38; // words per (cell, phase) window: 9 rows x 4 words + 2 (8-byte aligned rows)
+// One CTA per 32 consecutive level-0 cells of one (job, reference), 9 warps: in each step warp w
+// scores position w of the step (the centre first) for all 32 cells, a lane per cell, each lane
+// its cell's four 4x4 quarter-pel SATDs summed. The lanes of a load then read the same row of the
+// same tile for 32 neighbouring cells: where their MVs agree -- most of a frame -- that is one
+// contiguous run of a phase plane's row, a few cache lines per load (a lane per (cell, position,
+// tile) scattered each warp's loads over nine phase planes and was bound by the L1's wavefronts).
+// The cur tiles are row-transformed once per cell into shared memory, cell-minor so a warp's reads
+// are conflict-free; one thread per cell replays the centre-first strict choice.
+constexpr int kRefineCells = 32, kRefineWarps = 9, kRefineThreads = 32 * kRefineWarps;
 
-__global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
-  // per (cell, tile) its 16 row coefficients, 17 words apart: the tiles and cells one warp reads
-  // at once fall in different banks
-  __shared__ int cc[kRefineCells * 4][17];
-  __shared__ int sat[kRefineCells][9];
+__global__ void __launch_bounds__(kRefineThreads, 4) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
+  __shared__ int cc[4][16][kRefineCells];  // [tile][row coefficient][cell]
+  __shared__ int sat[kRefineWarps][kRefineCells];
   __shared__ int mvx[kRefineCells], mvy[kRefineCells], need[kRefineCells];
-  __shared__ int wx0[kRefineCells], wy0[kRefineCells];  // window origin: column (8-aligned), row
-  __shared__ __align__(16) uint32_t win[kRefineCells * kPhases * kRwStride];
   __shared__ int unit_slot;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int unit, iter = 0;
   while (take_unit(w, unit, iter, &unit_slot)) {
   const int jb = job_of(w, unit);
@@ -367,65 +357,55 @@ __global__ void __launch_bounds__(kRefineThreads, 5) k_me_refine(const FrameJob*
   const int ncells = min(kRefineCells, ncell - cell0);
   const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
   int* field = job.field[r][0];
-  if (tid < ncells * 16) {
-    const int c = tid >> 4, t = (tid >> 2) & 3, i = tid & 3;
-    const int cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
+  // the cur tiles' rows, row-transformed: (tile, row, cell) items, cells in lane order
+  for (int e = tid; e < 16 * kRefineCells; e += kRefineThreads) {
+    const int c = e & 31, t = e >> 7, i = (e >> 5) & 3;
+    const int cell = cell0 + min(c, ncells - 1), by = cell / cols, bx = cell - by * cols;
     const uint32_t cw = row4(cur, bx * 8 + 4 * (t & 1), by * 8 + 4 * (t >> 1) + i);
 #pragma unroll
-    for (int k = 0; k < 4; k++) cc[c * 4 + t][4 * k + i] = dp4a_us(cw, wh_row(k), 0);
+    for (int k = 0; k < 4; k++) cc[t][4 * k + i][c] = dp4a_us(cw, wh_row(k), 0);
   }
-  if (tid < ncells) {
-    const int m = field[cell0 + tid];
-    const int cell = cell0 + tid, by = cell / cols, bx = cell - by * cols;
+  if (tid < kRefineCells) {
+    const int cell = cell0 + min(tid, ncells - 1), by = cell / cols, bx = cell - by * cols;
+    const int m = field[cell];
     mvx[tid] = mv_x(m), mvy[tid] = mv_y(m);
-    need[tid] = cell_needed(job, r, bx, by);
-    wx0[tid] = (bx * 8 + (mv_x(m) >> 2) - 1) & ~7;
-    wy0[tid] = by * 8 + (mv_y(m) >> 2) - 1;
+    need[tid] = tid < ncells && cell_needed(job, r, bx, by);
   }
   // a unit none of whose cells a kept reference reads (pruned search): nothing to refine
-  if (!__syncthreads_or(tid < ncells && need[tid])) continue;
-  // 1. the windows: (phase, row, half) outer, cell inner (lane order); inside the stored plane as
-  //    asynchronous 8-byte copies (all in flight at once), else word by word with clamping
-  for (int e = tid; e < ncells * kPhases * kRwRows * 2; e += kRefineThreads) {
-    const int c = e % ncells, rest = e / ncells, half = rest & 1, row = (rest >> 1) % kRwRows, ph = (rest >> 1) / kRwRows;
-    if (!need[c]) continue;
-    DevPlane pp = ref;
-    pp.p = ref.p + (long long)ph * ref.phase;
-    const int x = wx0[c] + 8 * half, y = wy0[c] + row;
-    uint32_t* dst = win + (c * kPhases + ph) * kRwStride + row * 4 + 2 * half;
-    if (inside(pp, x, y, 8, 1)) {
-      cp_async8(dst, pp.p + (long long)y * pp.stride + x);
-    } else {
-      dst[0] = row4(pp, x, y), dst[1] = row4(pp, x + 4, y);
-    }
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  // 2. this thread's item (threads past the last item, or of a cell no superblock reads, work on
-  //    item 0 and drop the result)
-  const bool valid = tid < ncells * 36 && need[tid / 36];
-  const int it = valid ? tid : 0, c = it / 36, rem = it - c * 36, t = rem >> 2, tile = rem & 3;
-  const int n = refine_pos(t), cell = cell0 + c, by = cell / cols, bx = cell - by * cols;
-  const int tx0 = bx * 8 + 4 * (tile & 1) - wx0[c], ty0 = by * 8 + 4 * (tile >> 1) - wy0[c];
+  if (!__syncthreads_or(tid < kRefineCells && need[tid])) continue;
+  const int c = lane, n = refine_pos(warp);
+  const int cell = cell0 + min(c, ncells - 1), by = cell / cols, bx = cell - by * cols;
   for (int step = 2; step >= 1; step--) {
     const int qx = mvx[c] + (n % 3 - 1) * step, qy = mvy[c] + (n / 3 - 1) * step;
-    // the tile's rows in the window: byte b (0..12) of rows r0 .. r0 + 3 (r0 0..5)
-    const int b = tx0 + (qx >> 2), r0 = ty0 + (qy >> 2);
-    const uint32_t* wr = win + (c * kPhases + (qy & 3) * 4 + (qx & 3)) * kRwStride + r0 * 4 + (b >> 2);
-    const unsigned sh = (unsigned)(b & 3) * 8;
-    uint32_t pr[4];
+    DevPlane ph = ref;
+    ph.p = ref.p + (long long)((qy & 3) * 4 + (qx & 3)) * ref.phase;
+    const int x = bx * 8 + (qx >> 2), y = by * 8 + (qy >> 2);
+    const bool fast = inside(ph, x, y, 8, 8);
+    int v = 0;
 #pragma unroll
-    for (int i = 0; i < 4; i++) pr[i] = __funnelshift_r(wr[4 * i], wr[4 * i + 1], sh);
-    int v = satd4_rows(cc[c * 4 + tile], pr);  // the cur coefficients read from shared memory as used
-    v += __shfl_xor_sync(0xffffffffu, v, 1);
-    v += __shfl_xor_sync(0xffffffffu, v, 2);
-    if (valid && tile == 0) sat[c][t] = v;
+    for (int t = 0; t < 4; t++) {
+      const int tx = x + 4 * (t & 1), ty = y + 4 * (t >> 1);
+      uint32_t pr[4];
+      if (fast) {
+        const uint8_t* p = ph.p + (long long)ty * ph.stride + tx;
+#pragma unroll
+        for (int i = 0; i < 4; i++) pr[i] = load4(p + (long long)i * ph.stride);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; i++) pr[i] = row4(ph, tx, ty + i);
+      }
+      int C[16];
+#pragma unroll
+      for (int k = 0; k < 16; k++) C[k] = cc[t][k][c];
+      v += satd4_rows(C, pr);
+    }
+    sat[warp][c] = v;
     __syncthreads();
     if (tid < ncells && need[tid]) {
       const int cx = mvx[tid], cy = mvy[tid];
-      int best = sat[tid][0], nx = cx, ny = cy;
+      int best = sat[0][tid], nx = cx, ny = cy;
       for (int k = 1; k < 9; k++) {
-        const int s = sat[tid][k] + kSubpelPenalty, m = refine_pos(k);
+        const int s = sat[k][tid] + kSubpelPenalty, m = refine_pos(k);
         if (s < best) best = s, nx = cx + (m % 3 - 1) * step, ny = cy + (m / 3 - 1) * step;
       }
       mvx[tid] = nx, mvy[tid] = ny;
