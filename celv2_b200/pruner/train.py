@@ -9,12 +9,13 @@
    all four qindex values.
 2. Labels: per superblock the options the exhaustive decision's chosen partition uses (references,
    intra, block levels, intra modes; data.labels). Masks of exactly those options lose nothing.
+   (`--weights`: thresholds for weights trained before; steps 1-3 are skipped.)
 3. Adam on the weighted cross-entropy, with the library's own forward, backward, loss and Adam
    kernels.
 4. Thresholds: on the validation clips, the fastest setting (device time of the clips through the
    engine) whose summed chosen-partition cost rises by at most `--max-loss` (1 %) over the
-   exhaustive search; then the confidence band (the fallback to the full search) widened as far as
-   the budget allows.
+   exhaustive search, by a coordinate search over the four thresholds; then the confidence band
+   (the fallback to the full search) widened as far as the budget allows.
 5. Report: per qindex on the held-out clips, the cost increase and speed-up of the network, of the
    used-option masks (the ceiling: perfect masks, no loss) and of rules without the network (keep
    the k nearest references, intra or not, every level or only the small ones), and the fallback
@@ -54,32 +55,15 @@ def clips_in_chunks(pool, seeds, frames, chunk):
             yield s, c
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.dirname(WEIGHTS))
-    ap.add_argument("--clips", type=int, default=200)
-    ap.add_argument("--test-clips", type=int, default=20)
-    ap.add_argument("--steps", type=int, default=8000)
-    ap.add_argument("--batch", type=int, default=2048)
-    ap.add_argument("--max-loss", type=float, default=0.01)
-    ap.add_argument("--workers", type=int, default=max(1, min(16, (os.cpu_count() or 2) // 2)))
-    args = ap.parse_args()
-    t0 = time.time()
-    pool = mp.get_context("spawn").Pool(args.workers)  # spawned workers: no CUDA state inherited
-
+def train_network(eng, pool, seeds, args, t0):
+    """1-3: the records of the training clips and the network trained on them; returns (params,
+    the samples, the loss curve, the positive share per output)."""
     import torch
 
-    from .. import engine as E
     from .. import gop
 
-    eng = E.CudaEngine(1920, 1080)
-    eng.reserve_group(10)
-    eng.set_config(E.CFG_GRAPHS, 1)
-    plan17, plan33 = gop.stream_plan(17), gop.stream_plan(33)
-
-    # 1-2. training records
+    plan17 = gop.stream_plan(17)
     xs, ys, ws = [], [], []
-    seeds = list(range(TRAIN_SEED0, TRAIN_SEED0 + args.clips))
     for k, (seed, clip) in enumerate(clips_in_chunks(pool, seeds, 17, 2 * args.workers)):
         (x, y, w, _), _, _ = D.collect(eng, clip, QS[k % 4], plan17)
         xs.append(x), ys.append(y), ws.append(w)
@@ -108,6 +92,41 @@ def main():
     params = tr.params()
     del x, y, w
     torch.cuda.empty_cache()
+    return params, X, losses, positives
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=os.path.dirname(WEIGHTS))
+    ap.add_argument("--clips", type=int, default=200)
+    ap.add_argument("--test-clips", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=8000)
+    ap.add_argument("--batch", type=int, default=2048)
+    ap.add_argument("--max-loss", type=float, default=0.01)
+    ap.add_argument("--workers", type=int, default=max(1, min(16, (os.cpu_count() or 2) // 2)))
+    ap.add_argument("--weights", default=None,
+                    help="trained weights to choose thresholds for (skips the records and the training)")
+    args = ap.parse_args()
+    t0 = time.time()
+    pool = mp.get_context("spawn").Pool(args.workers)  # spawned workers: no CUDA state inherited
+
+    from .. import engine as E
+    from .. import gop
+
+    eng = E.CudaEngine(1920, 1080)
+    eng.reserve_group(10)
+    eng.set_config(E.CFG_GRAPHS, 1)
+    plan17, plan33 = gop.stream_plan(17), gop.stream_plan(33)
+
+    seeds = list(range(TRAIN_SEED0, TRAIN_SEED0 + args.clips))
+    if args.weights:
+        prev = json.load(open(os.path.join(os.path.dirname(args.weights), "report.json")))
+        params, X, losses, positives = np.load(args.weights)["params"], None, prev["loss_curve"], \
+            np.array(prev["positive_share"])
+    else:
+        params, X, losses, positives = train_network(eng, pool, seeds, args, t0)
+    samples = int(X.shape[0]) if X is not None else prev["samples"]
+    del X
 
     # 4. thresholds on the validation clips (each at one qindex)
     val = [(c, QS[i]) for i, (_, c) in enumerate(clips_in_chunks(pool, VAL_SEEDS, 17, len(VAL_SEEDS)))]
@@ -149,13 +168,36 @@ def main():
         return rows, used
 
     val_rows, val_used = baseline(val, plan17)
-    grid = [("net", a, b, c, d, 0.0) for a in (0.2, 0.35, 0.5, 0.65, 0.8) for b in (0.3, 0.5, 0.7, 0.9)
-            for c in (0.05, 0.1, 0.2, 0.35, 0.5) for d in (0.05, 0.15, 0.3)]
-    sweep = []
-    for s in grid:
-        sweep.append({"setting": list(s), **measure(val_rows, plan17, s)})
-    ok = [r for r in sweep if r["loss"] <= args.max_loss]
-    best = max(ok, key=lambda r: r["speedup"]) if ok else min(sweep, key=lambda r: r["loss"])
+    # coordinate search from a middle setting: each threshold over its range in turn, keeping the
+    # fastest setting within the budget (the least costly one while none is within it), two rounds
+    ranges = [(0.3, 0.5, 0.65, 0.8, 0.9, 0.95, 0.98), (0.3, 0.5, 0.7, 0.9, 0.95, 0.99),
+              (0.1, 0.2, 0.35, 0.5, 0.7, 0.85), (0.1, 0.2, 0.3, 0.5, 0.7)]
+    cur = [0.5, 0.5, 0.35, 0.3]
+    sweep, seen = [], {}
+
+    def score(th):
+        key = tuple(th)
+        if key not in seen:
+            r = {"setting": ["net", *th, 0.0], **measure(val_rows, plan17, ("net", *th, 0.0))}
+            seen[key] = r
+            sweep.append(r)
+        return seen[key]
+
+    def better(a, b):
+        fa, fb = a["loss"] <= args.max_loss, b["loss"] <= args.max_loss
+        if fa != fb:
+            return fa
+        return a["speedup"] > b["speedup"] if fa else a["loss"] < b["loss"]
+
+    best = score(cur)
+    for _ in range(2):
+        for i, rng in enumerate(ranges):
+            for v in rng:
+                th = list(cur)
+                th[i] = v
+                r = score(th)
+                if better(r, best):
+                    best, cur = r, th
     for band in (0.01, 0.02, 0.05):  # the fallback band: widest that keeps the budget and some speed
         s = tuple(best["setting"][:5]) + (band,)
         r = {"setting": list(s), **measure(val_rows, plan17, s)}
@@ -183,7 +225,7 @@ def main():
     os.makedirs(args.out, exist_ok=True)
     np.savez(os.path.join(args.out, "weights.npz"), params=params,
              **{k: np.float32(v) for k, v in chosen.items()})
-    report = {"samples": int(X.shape[0]), "clips": args.clips, "steps": args.steps, "batch": args.batch,
+    report = {"samples": samples, "clips": args.clips, "steps": args.steps, "batch": args.batch,
               "loss_curve": losses, "positive_share": positives.tolist(), "max_loss": args.max_loss,
               "chosen": best, "thresholds": chosen, "validation": sweep, "test_per_qindex": test,
               "seeds": {"train": [seeds[0], seeds[-1]], "val": VAL_SEEDS, "test": [test_seeds[0], test_seeds[-1]]},
