@@ -51,16 +51,22 @@ __device__ unsigned char g_cand_cell[kSlots];
 constexpr int kMaxRegions = 16;  // 16x16 regions of a superblock
 constexpr int kRegCells = 256;   // regions x neighbourhood cells at most (16 x 16, 4 x 36, 1 x 100)
 
+// Per candidate slot (in g_slot's order) and per block: level | 32x32 region << 2 | 16x16 region
+// << 4. The slots of one level are contiguous in g_slot's order: level l's from c_level_slot[l].
+__device__ unsigned char g_slot_aux[kSlots];
+__device__ unsigned char g_block_aux[kBlocks];
+__constant__ int c_level_slot[5];
+
 // The region pass's shared state.
 struct RegionSmem {
-  int nb[kNb];                 // packed MV of each neighbourhood cell
+  int rnb[kInterThreads];      // per thread (region, local cell): the cell's packed MV
   int D[kRegCells];            // per region r: its distinct MVs at D[r * ncell ..], first occurrence order
   int moff[kRegCells];         // per (region, MV): the superblock's prediction, bytes from the reference's level 0
   unsigned char mfast[kRegCells];  // per (region, MV): the region's prediction lies inside the margin
-  unsigned char first[kRegCells];  // per (region, cell): the cell holds the first occurrence of its MV
   unsigned char dmap[kMaxRegions][kNb];  // per region: neighbourhood cell -> its MV's index in the region's D
+  unsigned bal[kInterThreads / 32];      // per warp: which lanes hold a first occurrence
   int nd[kMaxRegions];
-  unsigned char list[kSlots];         // per candidate slot: its MV index in its region's D (255: pruned block)
+  int nd_max;
   unsigned key[kBlocks];              // per block: least (SATD << 7 | candidate index) so far
 };
 
@@ -316,80 +322,67 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
   }  // units
 }
 
-__global__ void __launch_bounds__(kInterThreads, 4) k_inter_regions(const FrameJob* __restrict__ jobs, WorkList w, int chunk) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  RegionSmem& S = *reinterpret_cast<RegionSmem*>(smem_raw);
-  const ChunkSums Q = chunk_sums(smem_raw, chunk);
-  __shared__ int unit_slot;
-  const int tid = threadIdx.x, lane = tid & 31;
-  int unit, iter = 0;
-  while (take_unit(w, unit, iter, &unit_slot)) {
-  const int jb = job_of(w, unit);
-  const FrameJob& job = jobs[jb];
-  const int nsb = job.sb_cols * job.sb_rows;
-  const int u = unit - w.prefix[jb];
-  const int r = u / nsb, sb = u - r * nsb, sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
-  const unsigned keep = keep_mask(job, sb);
-  // a pruned (superblock, reference) is not scored; with 64-level blocks k_inter scores it
-  if (!(keep >> r & 1u) || (keep & CELV2_KEEP_LEVEL(0))) continue;
+// One (superblock, reference) unit of the region pass, regions of R x R samples (32 or 16).
+template <int R>
+__device__ __forceinline__ void region_unit(RegionSmem& S, const ChunkSums& Q, const FrameJob& job, int r, int sb,
+                                            int sbx, int sby, unsigned keep, int chunk) {
+  constexpr int nr = 64 / R, nreg = nr * nr, rcells = R / 8, rc = rcells + 2, ncell = rc * rc;
+  constexpr int per = kInterThreads / nreg;  // threads per region: 64 (R = 32) or 16 (R = 16)
+  static_assert(per >= ncell && (per & (per - 1)) == 0 && nreg * ncell <= kRegCells, "region layout");
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int ox = sbx * 64, oy = sby * 64;
   const int cols = job.fcols[0], rows = job.frows[0];
   const int* field = job.field[r][0];
-  // regions: its 32x32 squares, or 16x16 ones where the 32-level blocks are pruned too
-  const int R = (keep & CELV2_KEEP_LEVEL(1)) ? 32 : 16;
-  const int nr = 64 / R, nreg = nr * nr, rc = R / 8 + 2, ncell = rc * rc;
 
-  // 1. neighbourhood MVs; per region the distinct MVs of its cells (first occurrence order) and
-  //    the map from its cells to them; the blocks' candidate lists
-  if (tid < kNb) {
-    const int ny = tid / 10, nx = tid - ny * 10;
-    const int cx = clampi(sbx * 8 - 1 + nx, 0, cols - 1), cy = clampi(sby * 8 - 1 + ny, 0, rows - 1);
-    S.nb[tid] = field[cy * cols + cx];
+  // 1. thread (region reg, local cell lc) reads its neighbourhood cell's MV (clamped into the field)
+  const int reg = tid / per, lc = tid % per;
+  const bool live = lc < ncell;
+  const int c10 = ((reg / nr) * rcells + lc / rc) * 10 + (reg % nr) * rcells + lc % rc;
+  int v = 0;
+  if (live) {
+    const int cx = clampi(sbx * 8 - 1 + c10 % 10, 0, cols - 1), cy = clampi(sby * 8 - 1 + c10 / 10, 0, rows - 1);
+    v = __ldg(field + cy * cols + cx);
   }
+  S.rnb[tid] = v;
   for (int b = tid; b < kBlocks; b += kInterThreads) S.key[b] = 0xffffffffu;
+  if (tid == 0) S.nd_max = 0;
   __syncthreads();
-  // thread e is local cell lc of region reg: neighbourhood cell c10
-  const int e = tid, reg = e / ncell, lc = e - reg * ncell;
-  const bool elive = e < nreg * ncell;
-  const int rx0 = (reg % nr) * (R / 8), ry0 = (reg / nr) * (R / 8);
-  const int c10 = (ry0 + lc / rc) * 10 + rx0 + lc % rc;
-  int firstlc = 0;  // the region's first local cell with this cell's MV
-  if (elive) {
-    const int v = S.nb[c10];
-    while (S.nb[(ry0 + firstlc / rc) * 10 + rx0 + firstlc % rc] != v) firstlc++;
-    S.first[e] = firstlc == lc;
+  // the region's first local cell holding this MV; the first occurrences, in local cell order, are
+  // the region's distinct MVs: an MV's index is the number of first occurrences before its own
+  int firstlc = lc;
+  if (live) {
+    const int* rn = S.rnb + reg * per;
+    for (int k = 0; k < lc; k++)
+      if (rn[k] == v) {
+        firstlc = k;
+        break;
+      }
   }
-  __syncthreads();
-  if (elive) {  // the MV's index in the region's D: the first occurrences before its own
-    int pos = 0;
-    for (int k = 0; k < firstlc; k++) pos += S.first[reg * ncell + k];
-    S.dmap[reg][c10] = (unsigned char)pos;
-    if (firstlc == lc) S.D[reg * ncell + pos] = S.nb[c10];
+  const bool is_first = live && firstlc == lc;
+  const unsigned bal = __ballot_sync(0xffffffffu, is_first);
+  if (lane == 0) S.bal[warp] = bal;
+  const int nd_sum = __syncthreads_count(is_first);
+  int pos, nd;
+  if constexpr (per == 16) {  // two regions per warp, a half each
+    const unsigned rb = (bal >> ((reg & 1) * 16)) & 0xffffu;
+    pos = __popc(rb & ((1u << firstlc) - 1u)), nd = __popc(rb);
+  } else {  // a region over two warps: local cells 0-31 and 32-35
+    const unsigned ba = S.bal[2 * reg], bb = S.bal[2 * reg + 1];
+    pos = firstlc < 32 ? __popc(ba & ((1u << firstlc) - 1u)) : __popc(ba) + __popc(bb & ((1u << (firstlc - 32)) - 1u));
+    nd = __popc(ba) + __popc(bb);
   }
-  if (tid < nreg) {
-    int n = 0;
-    for (int k = 0; k < ncell; k++) n += S.first[tid * ncell + k];
-    S.nd[tid] = n;
-  }
-  __syncthreads();
+  if (live) S.dmap[reg][c10] = (unsigned char)pos;
   const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
-  if (elive && lc < S.nd[reg]) {  // per (region, MV): the prediction's offset, inside the margin or not
-    const int m = S.D[e], mx = mv_x(m), my = mv_y(m);
+  if (is_first) {  // per (region, MV): the prediction's offset, inside the margin or not
+    const int e = reg * ncell + pos, mx = mv_x(v), my = mv_y(v);
     const int x = ox + (mx >> 2), y = oy + (my >> 2);
     const long long o = (long long)((my & 3) * 4 + (mx & 3)) * ref.phase + (long long)y * ref.stride + x;
+    S.D[e] = v;
     S.moff[e] = (int)o;
     S.mfast[e] = inside(ref, x + (reg % nr) * R, y + (reg / nr) * R, R, R) && o == (long long)(int)o;
   }
-  int nd_max = 0, nd_sum = 0;
-  for (int k = 0; k < nreg; k++) nd_max = max(nd_max, S.nd[k]), nd_sum += S.nd[k];
+  if (lc == 0) S.nd[reg] = nd, atomicMax(&S.nd_max, nd);
   if (tid == 0 && job.stats) atomicAdd(job.stats + kStatInterMvs, (unsigned long long)nd_sum * (R / 4) * (R / 4));
-  for (int k = tid; k < kSlots; k += kInterThreads) {
-    const unsigned bp = g_slot[k];
-    const int b = bp & 511;
-    int bx, by, bw, bh;
-    sb_block_geom(b, bx, by, bw, bh);
-    S.list[k] = (keep & CELV2_KEEP_LEVEL(block_level(b))) ? S.dmap[(by / R) * nr + bx / R][bp >> 16] : (unsigned char)255;
-  }
 
   // this thread's tile: its cur rows, row-transformed, in registers (the grid lies inside the margin)
   const int tx = tid & 15, ty = tid >> 4;
@@ -404,22 +397,27 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter_regions(const FrameJ
   // the tile's prediction rows at MV d start at tile_base + moff[d]; words a row apart are ws apart
   const uintptr_t tile_base = reinterpret_cast<uintptr_t>(ref.p) + (uintptr_t)(ty * 4 * ref.stride + tx * 4);
   const int ws = ref.stride >> 2;  // strides are multiples of 64
-  __syncthreads();  // lists, offsets complete
-  const int tnd = S.nd[treg], tbase = treg * ncell;
-  // chunks of equal size, at most `chunk` MVs each (a region's MVs past its count are not scored)
+  __syncthreads();  // MVs, maps, offsets complete
+  const int tnd = S.nd[treg], tbase = treg * ncell, nd_max = S.nd_max;
+  const int wnd = __reduce_max_sync(0xffffffffu, tnd);  // the most MVs of this warp's regions
+  // the candidate slots of the kept levels (contiguous by level in g_slot's order; levels 1-3 here)
+  const unsigned lv = (keep & CELV2_KEEP_LEVELS) >> 8;
+  const int slot_lo = c_level_slot[__ffs(lv) - 1], slot_hi = c_level_slot[32 - __clz(lv)];
+  // chunks of equal size, at most `chunk` MVs each
   const int nchunks = (nd_max + chunk - 1) / chunk, csize = (nd_max + nchunks - 1) / nchunks;
 
   for (int c0 = 0; c0 < nd_max; c0 += csize) {
     const int nc = min(csize, nd_max - c0);
     const int tnc = min(nc, tnd - c0);  // this tile's region's MVs in the chunk
-    // 2. tile SATDs at every MV of the chunk (two MVs per step for load parallelism); an 8x8
-    //    cell's tiles are lanes l, l + 1, l + 16, l + 17 of one warp (and of one region)
-    for (int dd = 0; dd < nc; dd += 2) {
+    const int wnc = min(nc, wnd - c0);  // this warp's
+    // 2. tile SATDs at the region's MVs of the chunk (two MVs per step for load parallelism); an
+    //    8x8 cell's tiles are lanes l, l + 1, l + 16, l + 17 of one warp (and of one region)
+    for (int dd = 0; dd < wnc; dd += 2) {
       int sat[2];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        // a region with no MV left in this chunk scores its first MV (always there) and its
-        // sums are never read: its slots name only its own MVs
+        // a tile whose region has no MV left scores its region's first MV (always there); those
+        // sums are never read: a region's slots name only its own MVs
         const int d = tbase + (tnc > 0 ? c0 + min(dd + h, tnc - 1) : 0);
         uint32_t pr[4];
         if (S.mfast[d]) {  // the usual case: rows from aligned words
@@ -449,41 +447,65 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter_regions(const FrameJ
       }
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        int v = sat[h] + __shfl_xor_sync(0xffffffffu, sat[h], 1);
-        v += __shfl_xor_sync(0xffffffffu, v, 16);
-        if (dd + h < nc) {
+        int v8 = sat[h] + __shfl_xor_sync(0xffffffffu, sat[h], 1);
+        v8 += __shfl_xor_sync(0xffffffffu, v8, 16);
+        if (dd + h < wnc) {
           Q.tile[dd + h][tid] = (unsigned short)sat[h];
-          if (lane < 16 && !(lane & 1)) Q.whole8[dd + h][(tid >> 5) * 8 + (lane >> 1)] = (unsigned short)v;
+          if (lane < 16 && !(lane & 1)) Q.whole8[dd + h][(tid >> 5) * 8 + (lane >> 1)] = (unsigned short)v8;
         }
       }
     }
     __syncthreads();
+    // 16x16 sums (a 16x16 square lies in one region, so its four 8x8 sums exist wherever it is read)
     for (int k = tid; k < nc * 16; k += kInterThreads) {
       const int dd = k >> 4, i = k & 15, c = (i >> 2) * 16 + (i & 3) * 2;
       const unsigned short* W = Q.whole8[dd];
       Q.sum16[dd][i] = W[c] + W[c + 1] + W[c + 8] + W[c + 9];
     }
     __syncthreads();
-    // 3. every candidate slot whose MV is in this chunk (the slot's region's MVs)
-    for (int k = tid; k < kSlots; k += kInterThreads) {
-      const int d = (int)S.list[k] - c0;
-      if (d < 0 || d >= nc) continue;  // 255: a pruned block
-      const unsigned bp = g_slot[k];
-      const int b = bp & 511, kk = (bp >> 9) & 127;
-      atomicMin(&S.key[b], ((unsigned)block_satd(Q, b, d) << 7) | (unsigned)kk);
+    // 3. every candidate slot of a kept level whose MV (in its block's region) is in this chunk
+    for (int k = slot_lo + tid; k < slot_hi; k += kInterThreads) {
+      const unsigned aux = __ldg(g_slot_aux + k);
+      if (!(keep & CELV2_KEEP_LEVEL(aux & 3u))) continue;
+      const unsigned bp = __ldg(g_slot + k);
+      const int d = (int)S.dmap[R == 32 ? (aux >> 2) & 3u : aux >> 4][bp >> 16] - c0;
+      if (d < 0 || d >= nc) continue;
+      const int b = bp & 511;
+      atomicMin(&S.key[b], ((unsigned)block_satd(Q, b, d) << 7) | ((bp >> 9) & 127u));
     }
     __syncthreads();  // the next chunk overwrites the sums
   }
   int2* out = job.inter + ((long long)sb * kMaxRefs + r) * kBlocks;
   for (int b = tid; b < kBlocks; b += kInterThreads) {
-    if (!(keep & CELV2_KEEP_LEVEL(block_level(b)))) continue;  // a pruned block: never read
-    int bx, by, bw, bh;
-    sb_block_geom(b, bx, by, bw, bh);
-    const int breg = (by / R) * nr + bx / R;
+    const unsigned aux = __ldg(g_block_aux + b);
+    if (!(keep & CELV2_KEEP_LEVEL(aux & 3u))) continue;  // a pruned block: never read
+    const int breg = R == 32 ? (aux >> 2) & 3u : aux >> 4;
     const unsigned k = S.key[b];
     out[b] = make_int2((int)(k >> 7), S.D[breg * ncell + S.dmap[breg][g_cand_cell[c_cand_off[b] + (k & 127)]]]);
   }
-  }  // units
+}
+
+__global__ void __launch_bounds__(kInterThreads, 4) k_inter_regions(const FrameJob* __restrict__ jobs, WorkList w, int chunk) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  RegionSmem& S = *reinterpret_cast<RegionSmem*>(smem_raw);
+  const ChunkSums Q = chunk_sums(smem_raw, chunk);
+  __shared__ int unit_slot;
+  int unit, iter = 0;
+  while (take_unit(w, unit, iter, &unit_slot)) {
+    const int jb = job_of(w, unit);
+    const FrameJob& job = jobs[jb];
+    const int nsb = job.sb_cols * job.sb_rows;
+    const int u = unit - w.prefix[jb];
+    const int r = u / nsb, sb = u - r * nsb, sby = sb / job.sb_cols, sbx = sb - sby * job.sb_cols;
+    const unsigned keep = keep_mask(job, sb);
+    // a pruned (superblock, reference) is not scored; with 64-level blocks k_inter scores it
+    if (!(keep >> r & 1u) || (keep & CELV2_KEEP_LEVEL(0))) continue;
+    // regions: its 32x32 squares, or 16x16 ones where the 32-level blocks are pruned too
+    if (keep & CELV2_KEEP_LEVEL(1))
+      region_unit<32>(S, Q, job, r, sb, sbx, sby, keep, chunk);
+    else
+      region_unit<16>(S, Q, job, r, sb, sbx, sby, keep, chunk);
+  }
 }
 
 void launch_inter(const FrameJob* jobs, const WorkList& w, int chunk, bool regions, unsigned* region_queue,
@@ -523,8 +545,29 @@ cudaError_t inter_attributes() {
   }
   if (o != kSlots) return cudaErrorInvalidValue;
   std::sort(order, order + kSlots);
-  for (int e = 0; e < kSlots; e++) slot[e] = (unsigned)order[e];
+  // level | 32x32 region << 2 | 16x16 region << 4 of a block (its region: where its top-left lies)
+  auto aux_of = [](int b) {
+    int x, y, w, h;
+    sb_block_geom(b, x, y, w, h);
+    return (unsigned char)(block_level(b) | ((y / 32) * 2 + x / 32) << 2 | ((y / 16) * 4 + x / 16) << 4);
+  };
+  static unsigned char slot_aux[kSlots];
+  unsigned char block_aux[kBlocks];
+  int level_slot[5] = {0, 0, 0, 0, kSlots};
+  for (int b = 0; b < kBlocks; b++) block_aux[b] = aux_of(b);
+  for (int e = 0; e < kSlots; e++) {
+    slot[e] = (unsigned)order[e];
+    slot_aux[e] = block_aux[slot[e] & 511];
+  }
+  for (int l = 1; l < 4; l++) {  // the first slot of level l (the slots are ordered by level)
+    int e = 0;
+    while (e < kSlots && (slot_aux[e] & 3) < l) e++;
+    level_slot[l] = e;
+  }
   cudaError_t e = cudaMemcpyToSymbol(c_cand_off, off, sizeof off);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_slot_aux, slot_aux, sizeof slot_aux);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_block_aux, block_aux, sizeof block_aux);
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_level_slot, level_slot, sizeof level_slot);
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_cand_cell, cell, sizeof cell);
   if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_slot, slot, sizeof slot);
   if (e != cudaSuccess) return e;

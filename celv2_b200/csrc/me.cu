@@ -226,8 +226,11 @@ __global__ void __launch_bounds__(kMeThreads, 4) k_me_level(const FrameJob* __re
   cp_async_wait_all();
   __syncthreads();
 
-  // ---- C. +-8 search (me_search, inter_common.h:108-119): a thread per (search, dx) ----
-  for (int item = tid; item < nsearch * 17; item += kMeThreads) {
+  // ---- C. +-8 search (me_search, inter_common.h:108-119): a thread per (search, dx), then a
+  //      thread per (merged search, union column), in one loop so the two kinds share rounds ----
+  const int nplain = nsearch * 17, nitems = nplain + nmerged * kUnion;
+  for (int item = tid; item < nitems; item += kMeThreads) {
+    if (item < nplain) {
     const int s = item / 17, dx = item - s * 17;
     const uint32_t* c = S.cur[S.scell[s]];
     uint32_t cw[16];
@@ -258,16 +261,15 @@ __global__ void __launch_bounds__(kMeThreads, 4) k_me_level(const FrameJob* __re
       best = key < best ? key : best;
     }
     atomicMin(&S.skey[s], best);
-  }
-  // merged searches: a thread per union column (at most 19); every union position's SAD is the
-  // same for both centres, and each centre takes its own penalty and raster index -- the same keys
-  // as its own 17 x 17 search, so the same first strict minimum
-  for (int item = tid; item < nmerged * kUnion; item += kMeThreads) {
-    const int m = item / kUnion, du = item - m * kUnion, s = MeSmem<CELLS>::kSearches - 1 - m;
+    } else {
+    // merged searches: a thread per union column (at most 19); every union position's SAD is the
+    // same for both centres, and each centre takes its own penalty and raster index -- the same
+    // keys as its own 17 x 17 search, so the same first strict minimum. All 19 union rows are
+    // summed (fixed trip counts; rows past the centres' union are never keyed)
+    const int m = (item - nplain) / kUnion, du = item - nplain - m * kUnion, s = MeSmem<CELLS>::kSearches - 1 - m;
     const int cx1 = S.sx[s], cy1 = S.sy[s], cx2 = S.sx2[s], cy2 = S.sy2[s];
     const int ux = min(cx1, cx2), uy = min(cy1, cy2);  // union position 0 = centre offset -8
     if (du >= 17 + abs(cx1 - cx2)) continue;
-    const int nrow = 17 + abs(cy1 - cy2);
     const uint32_t* c = S.cur[S.scell[s]];
     uint32_t cw[16];
 #pragma unroll
@@ -285,8 +287,7 @@ __global__ void __launch_bounds__(kMeThreads, 4) k_me_level(const FrameJob* __re
 #pragma unroll
       for (int i = 0; i < 8; i++) {
         const int dy = rr - i;
-        if (dy >= 0 && dy < kUnion && dy < nrow)
-          acc[dy] = sad4_acc(cw[2 * i + 1], w1, sad4_acc(cw[2 * i], w0, acc[dy]));
+        if (dy >= 0 && dy < kUnion) acc[dy] = sad4_acc(cw[2 * i + 1], w1, sad4_acc(cw[2 * i], w0, acc[dy]));
       }
     }
 #pragma unroll
@@ -300,12 +301,13 @@ __global__ void __launch_bounds__(kMeThreads, 4) k_me_level(const FrameJob* __re
 #pragma unroll
       for (int du_y = 0; du_y < kUnion; du_y++) {
         const int dy = oy + du_y;
-        if (du_y >= nrow || dy < 0 || dy > 16) continue;
+        if (dy < 0 || dy > 16) continue;
         const unsigned cost = acc[du_y] + pen_x + kMePenalty * abs(dy - kMeRange);
         const unsigned key = (cost << 9) | (unsigned)(dy * 17 + dx);
         best = key < best ? key : best;
       }
       atomicMin(t ? &S.skey2[s] : &S.skey[s], best);
+    }
     }
   }
   __syncthreads();
