@@ -332,22 +332,22 @@ __global__ void __launch_bounds__(kMeThreads, 4) k_me_level(const FrameJob* __re
 }
 
 // ---- quarter-pel refinement of level 0 (me_refine, inter_common.h:141-154) ----
-// One CTA per 32 consecutive level-0 cells of one (job, reference), 9 warps: in each step warp w
-// scores position w of the step (the centre first) for all 32 cells, a lane per cell, each lane
-// its cell's four 4x4 quarter-pel SATDs summed. The lanes of a load then read the same row of the
-// same tile for 32 neighbouring cells: where their MVs agree -- most of a frame -- that is one
-// contiguous run of a phase plane's row, a few cache lines per load (a lane per (cell, position,
-// tile) scattered each warp's loads over nine phase planes and was bound by the L1's wavefronts).
-// The cur tiles are row-transformed once per cell into shared memory, cell-minor so a warp's reads
-// are conflict-free; one thread per cell replays the centre-first strict choice.
-constexpr int kRefineCells = 32, kRefineWarps = 9, kRefineThreads = 32 * kRefineWarps;
+// One CTA per 32 consecutive level-0 cells of one (job, reference), 4 warps: warp t holds tile t
+// of the cells' four 4x4 tiles, a lane per cell, the cur tile row-transformed once into registers.
+// In each step a lane scores its tile at the step's nine positions; the lanes of a load read the
+// same row of the same tile for 32 neighbouring cells, which where their MVs agree -- most of a
+// frame -- is one contiguous run of a phase plane's row (a lane per (cell, position, tile)
+// scattered each warp's loads over nine phase planes and was bound by the L1's wavefronts; a warp
+// per position re-read the cur coefficients from shared memory nine times a step). The four tiles'
+// SATDs meet in shared memory and every lane replays its cell's centre-first strict choice from
+// them (the same in all four warps, so one barrier per step). The second step's centre is the
+// first step's winner, whose SATD the first step has already computed.
+constexpr int kRefineCells = 32, kRefineTiles = 4, kRefineThreads = 32 * kRefineTiles;
 
-__global__ void __launch_bounds__(kRefineThreads, 4) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
-  __shared__ int cc[4][16][kRefineCells];  // [tile][row coefficient][cell]
-  __shared__ int sat[kRefineWarps][kRefineCells];
-  __shared__ int mvx[kRefineCells], mvy[kRefineCells], need[kRefineCells];
+__global__ void __launch_bounds__(kRefineThreads, 7) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
+  __shared__ int sat[2][9][kRefineTiles][kRefineCells];  // [step][position][tile][cell]
   __shared__ int unit_slot;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, c = tid & 31, t = tid >> 5;
   int unit, iter = 0;
   while (take_unit(w, unit, iter, &unit_slot)) {
   const int jb = job_of(w, unit);
@@ -357,64 +357,58 @@ __global__ void __launch_bounds__(kRefineThreads, 4) k_me_refine(const FrameJob*
   const int u = unit - w.prefix[jb];
   const int r = u / groups, cell0 = (u - r * groups) * kRefineCells;
   const int ncells = min(kRefineCells, ncell - cell0);
+  const int cell = cell0 + min(c, ncells - 1), by = cell / cols, bx = cell - by * cols;
+  const bool need = c < ncells && cell_needed(job, r, bx, by);
+  // a unit none of whose cells a kept reference reads (pruned search): nothing to refine
+  if (!__syncthreads_or(need)) continue;
   const DevPlane cur = job.cur.lv[0], ref = job.ref[r].lv[0];
   int* field = job.field[r][0];
-  // the cur tiles' rows, row-transformed: (tile, row, cell) items, cells in lane order
-  for (int e = tid; e < 16 * kRefineCells; e += kRefineThreads) {
-    const int c = e & 31, t = e >> 7, i = (e >> 5) & 3;
-    const int cell = cell0 + min(c, ncells - 1), by = cell / cols, bx = cell - by * cols;
-    const uint32_t cw = row4(cur, bx * 8 + 4 * (t & 1), by * 8 + 4 * (t >> 1) + i);
+  // this lane's tile of its cell: origin, cur rows row-transformed
+  const int ox = bx * 8 + 4 * (t & 1), oy = by * 8 + 4 * (t >> 1);
+  int C[16];
+  {
+    uint32_t cw[4];
 #pragma unroll
-    for (int k = 0; k < 4; k++) cc[t][4 * k + i][c] = dp4a_us(cw, wh_row(k), 0);
+    for (int i = 0; i < 4; i++) cw[i] = row4(cur, ox, oy + i);
+    wh_rows_cur(cw, C);
   }
-  if (tid < kRefineCells) {
-    const int cell = cell0 + min(tid, ncells - 1), by = cell / cols, bx = cell - by * cols;
-    const int m = field[cell];
-    mvx[tid] = mv_x(m), mvy[tid] = mv_y(m);
-    need[tid] = tid < ncells && cell_needed(job, r, bx, by);
-  }
-  // a unit none of whose cells a kept reference reads (pruned search): nothing to refine
-  if (!__syncthreads_or(tid < kRefineCells && need[tid])) continue;
-  const int c = lane, n = refine_pos(warp);
-  const int cell = cell0 + min(c, ncells - 1), by = cell / cols, bx = cell - by * cols;
-  for (int step = 2; step >= 1; step--) {
-    const int qx = mvx[c] + (n % 3 - 1) * step, qy = mvy[c] + (n / 3 - 1) * step;
-    DevPlane ph = ref;
-    ph.p = ref.p + (long long)((qy & 3) * 4 + (qx & 3)) * ref.phase;
-    const int x = bx * 8 + (qx >> 2), y = by * 8 + (qy >> 2);
-    const bool fast = inside(ph, x, y, 8, 8);
-    int v = 0;
+  const int m = field[cell];
+  int cx = mv_x(m), cy = mv_y(m);  // quarter pels
+  int centre = 0;                  // the centre's SATD (the cell's four tiles), once known
 #pragma unroll
-    for (int t = 0; t < 4; t++) {
-      const int tx = x + 4 * (t & 1), ty = y + 4 * (t >> 1);
+  for (int s = 0; s < 2; s++) {
+    const int step = 2 - s;
+#pragma unroll
+    for (int k = s; k < 9; k++) {  // the second step's centre (k = 0) is the first step's winner
+      const int n = refine_pos(k);
+      const int qx = cx + (n % 3 - 1) * step, qy = cy + (n / 3 - 1) * step;
+      DevPlane ph = ref;
+      ph.p = ref.p + (long long)((qy & 3) * 4 + (qx & 3)) * ref.phase;
+      const int x = ox + (qx >> 2), y = oy + (qy >> 2);
       uint32_t pr[4];
-      if (fast) {
-        const uint8_t* p = ph.p + (long long)ty * ph.stride + tx;
+      if (inside(ph, x, y, 4, 4)) {
+        const uint8_t* p = ph.p + (long long)y * ph.stride + x;
 #pragma unroll
         for (int i = 0; i < 4; i++) pr[i] = load4(p + (long long)i * ph.stride);
       } else {
 #pragma unroll
-        for (int i = 0; i < 4; i++) pr[i] = row4(ph, tx, ty + i);
+        for (int i = 0; i < 4; i++) pr[i] = row4(ph, x, y + i);
       }
-      int C[16];
+      sat[s][k][t][c] = satd4_rows(C, pr);
+    }
+    __syncthreads();
+    // the cell's choice (me_refine: the centre first, a move must save kSubpelPenalty)
+    int best = s == 0 ? sat[0][0][0][c] + sat[0][0][1][c] + sat[0][0][2][c] + sat[0][0][3][c] : centre;
+    int raw = best, nx = cx, ny = cy;
 #pragma unroll
-      for (int k = 0; k < 16; k++) C[k] = cc[t][k][c];
-      v += satd4_rows(C, pr);
+    for (int k = 1; k < 9; k++) {
+      const int v = sat[s][k][0][c] + sat[s][k][1][c] + sat[s][k][2][c] + sat[s][k][3][c];
+      const int n = refine_pos(k);
+      if (v + kSubpelPenalty < best) best = v + kSubpelPenalty, raw = v, nx = cx + (n % 3 - 1) * step, ny = cy + (n / 3 - 1) * step;
     }
-    sat[warp][c] = v;
-    __syncthreads();
-    if (tid < ncells && need[tid]) {
-      const int cx = mvx[tid], cy = mvy[tid];
-      int best = sat[0][tid], nx = cx, ny = cy;
-      for (int k = 1; k < 9; k++) {
-        const int s = sat[k][tid] + kSubpelPenalty, m = refine_pos(k);
-        if (s < best) best = s, nx = cx + (m % 3 - 1) * step, ny = cy + (m / 3 - 1) * step;
-      }
-      mvx[tid] = nx, mvy[tid] = ny;
-    }
-    __syncthreads();
+    centre = raw, cx = nx, cy = ny;
   }
-  if (tid < ncells && need[tid]) field[cell0 + tid] = pack_mv(mvx[tid], mvy[tid]);
+  if (t == 0 && need) field[cell] = pack_mv(cx, cy);
   }  // units
 }
 
