@@ -857,13 +857,17 @@ struct celv2_engine {
     if (s.ready_pending) CK(cudaStreamWaitEvent(stream, s.ready, 0));
   }
 
-  // The slots a launch on `stream` reads: a later upload into them waits for this point.
+  // The slots a launch on `stream` reads: a later upload into them waits for this point. Their
+  // recency (`used`) becomes this launch's, so an upload into a dropped slot takes the one whose
+  // last reader was queued longest ago -- the one least likely to make the upload stream wait for
+  // work still in flight (the slots of the batch just queued are the most recent).
   void mark_used(Slot* const* slots, int n, cudaStream_t stream) {
     for (int i = 0; i < n; i++) {
       Slot* x = slots[i];
       if (!x->last_use) continue;  // not a store slot (launch()'s own cache, on this stream)
       CK(cudaEventRecord(x->last_use, stream));
       x->use_pending = true;
+      x->used = launches;
     }
   }
 
@@ -930,30 +934,29 @@ struct celv2_engine {
   }
 
   // ---- CUDA graphs: a batch's whole stage sequence captured once per shape, then replayed ----
+  // The descriptors are not part of the graph: each replay is preceded by their copy into djobs
+  // through the pinned ring (stream order puts it after the previous batch's kernels), so a replay
+  // never waits on the host for an earlier replay of the same graph.
   struct Graph {
     std::vector<int> key;  // each job's reference count
     cudaGraphExec_t exec = nullptr;
-    FrameJob* host_jobs = nullptr;  // pinned: the replay's descriptor copy reads it
-    cudaEvent_t done = nullptr;
-    bool replayed = false;
     int kernels = 0;
   };
   bool use_graphs = false;
   std::vector<Graph> graphs;
 
   void free_graphs() {
-    for (Graph& gr : graphs) {
+    for (Graph& gr : graphs)
       if (gr.exec) cudaGraphExecDestroy(gr.exec);
-      if (gr.host_jobs) cudaFreeHost(gr.host_jobs);
-      if (gr.done) cudaEventDestroy(gr.done);
-    }
     graphs.clear();
   }
 
   void launch_graph(const std::vector<FrameJob>& jobs, const std::vector<NetJob>& nets) {
+    // the shape: per job its reference count, whether it has keep words (which decides whether the
+    // region pass of the inter stage is launched at all), features and the network
     std::vector<int> key;
     for (size_t j = 0; j < jobs.size(); j++)
-      key.push_back(jobs[j].nrefs * 4 + (nets[j].feats ? 2 : 0) + (nets[j].net ? 1 : 0));
+      key.push_back(jobs[j].nrefs * 8 + (jobs[j].keep ? 4 : 0) + (nets[j].feats ? 2 : 0) + (nets[j].net ? 1 : 0));
     Graph* gr = nullptr;
     for (Graph& x : graphs)
       if (x.key == key) gr = &x;
@@ -962,12 +965,9 @@ struct celv2_engine {
       graphs.emplace_back();
       gr = &graphs.back();
       gr->key = key;
-      CK(cudaMallocHost(&gr->host_jobs, kMaxJobs * sizeof(FrameJob)));
-      CK(cudaEventCreateWithFlags(&gr->done, cudaEventDisableTiming));
       cudaGraph_t graph = nullptr;
       CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       try {
-        CK(cudaMemcpyAsync(djobs, gr->host_jobs, n * sizeof(FrameJob), cudaMemcpyHostToDevice, st));
         gr->kernels = enqueue_stages(jobs, true, st, nets);
       } catch (...) {
         cudaStreamEndCapture(st, &graph);
@@ -980,11 +980,8 @@ struct celv2_engine {
       cudaGraphDestroy(graph);
       CK(e);
     }
-    if (gr->replayed) CK(cudaEventSynchronize(gr->done));  // the last replay has read host_jobs
-    std::memcpy(gr->host_jobs, jobs.data(), n * sizeof(FrameJob));
+    put_jobs(jobs.data(), n, djobs, st);
     CK(cudaGraphLaunch(gr->exec, st));
-    CK(cudaEventRecord(gr->done, st));
-    gr->replayed = true;
     kernel_launches += gr->kernels;
   }
 };
@@ -1350,7 +1347,7 @@ int celv2_clear_store(celv2_engine* e) {
 int celv2_drop_frame(celv2_engine* e, long long key) {
   return guarded([&] {
     if (!e) invalid("null engine");
-    if (Slot* s = e->find(key)) s->key = -1, s->used = 0, s->resident = false;
+    if (Slot* s = e->find(key)) s->key = -1, s->resident = false;  // keeps its recency (`used`)
   });
 }
 

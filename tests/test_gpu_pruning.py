@@ -103,3 +103,30 @@ def test_region_scoring_at_1080p(oracle, graphs):
         # the used options lose nothing (a block of the chosen partition keeps its choice; a pruned
         # reference can only change which second reference a compound tries, never raise a cost)
         assert (e.sb_costs(0) <= full_cost).all()
+
+
+def test_masked_replay_after_an_exhaustive_capture(oracle):
+    """With CUDA graphs, a batch of one shape first decided exhaustively (its graph captured with no
+    keep words, so without the region pass of the inter stage) and then, on another frame, with
+    keep words that prune the 64-level blocks: the masked batch must not replay the exhaustive
+    graph, whose inter stage would leave the region units unscored."""
+    w, h = 416, 240
+    clip = synth.small_clip(seed=21, frames=6)
+    with E.CudaEngine(w, h) as e:
+        e.set_config(E.CFG_GRAPHS, 1)
+        for i, f in enumerate(clip):
+            e.upload(f.hy, i)
+        nsb = e.sb_cols * e.sb_rows
+        for _ in range(2):  # captured, then replayed
+            e.launch_group([5], [[4, 3, 2, 1]], 130, to_host=True)
+        want, _ = oracle.decide_masked(w, h, clip[5].y, [clip[r].y for r in (4, 3, 2, 1)], lam.lambda_q8(130))
+        assert records_equal(e.group_records(0), want)
+        keep = np.full(nsb, 0x0F | 0x80 | 0xE00, np.uint32)  # every reference and intra, no 64-level blocks
+        for _ in range(2):
+            e.set_keep(0, keep)
+            e.launch_group([4], [[3, 2, 1, 0]], 130, to_host=True)
+            want, want_cost = oracle.decide_masked(w, h, clip[4].y, [clip[r].y for r in (3, 2, 1, 0)],
+                                                   lam.lambda_q8(130), keep)
+            got = e.group_records(0)
+            assert records_equal(got, want), first_difference(got, want)
+            assert (e.sb_costs(0) == want_cost).all()
