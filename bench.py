@@ -340,6 +340,43 @@ def timed_on(stream, run, steps: int, dist, local) -> float:
     return max_over_ranks(a.elapsed_time(b), dist, local)
 
 
+def used_option_ceiling(eng, plan, args, stream, dist, local, world, full):
+    """(frames/s, cost increase) of the engine given, per superblock, the keep word of exactly the
+    options its exhaustive partition uses -- the words a perfect pruner would write -- timed like
+    the plain and the learned-pruned runs (the words go in through celv2_set_keep_words)."""
+    from celv2_b200.pruner.data import used_options
+
+    words = {}
+    for c in range(N_CLIPS):
+        for group in plan:
+            eng.launch_group([clip_key(c, s) for s, _ in group], [[clip_key(c, r) for r in refs] for _, refs in group],
+                             QINDEX, to_host=True)
+            for j, (s, refs) in enumerate(group):
+                if refs:
+                    words[(c, s)] = used_options(eng.group_records(j), len(refs))
+    costs = {}
+
+    def step(collect=False):
+        for c in range(N_CLIPS):
+            for group in plan:
+                for j, (s, refs) in enumerate(group):
+                    if refs:
+                        eng.set_keep(j, words[(c, s)])
+                launch_clip_group(eng, c, group)
+                if collect:
+                    for j, (s, refs) in enumerate(group):
+                        if refs:
+                            costs[(c, s)] = eng.sb_costs(j)
+
+    step(True)
+    for _ in range(max(1, args.warmup)):
+        step()
+    eng.finish()
+    ms = timed_on(stream, step, args.steps, dist, local)
+    loss = sum(float(v.sum()) for v in costs.values()) / sum(float(full[k].sum()) for k in costs) - 1.0
+    return NFRAMES * N_CLIPS * args.steps * world / (ms / 1e3), loss
+
+
 def run_pruned(eng, plan, args, stream, dist, local, world, plain_value):
     """The learned-pruned engine (celv2_set_pruner with the committed weights and thresholds) on
     the same mini-GOPs: frames/s timed like `value`, its speed-up, and what it costs -- the summed
@@ -389,6 +426,7 @@ def run_pruned(eng, plan, args, stream, dist, local, world, plain_value):
         eng.set_pruner(None)
     value = NFRAMES * N_CLIPS * args.steps * world / (ms / 1e3)
     loss = sum(float(v.sum()) for v in pruned.values()) / sum(float(full[k].sum()) for k in pruned) - 1.0
+    ceiling = used_option_ceiling(eng, plan, args, stream, dist, local, world, full)
     from celv2_b200.pruner import evaluate as V
 
     work = V.kept_work({k: m for k, (m, _) in kept.items()}, [[(k, [0] * n) for k, (_, n) in kept.items()]])
@@ -396,6 +434,10 @@ def run_pruned(eng, plan, args, stream, dist, local, world, plain_value):
     inter_sbs = nsb * sum(1 for g in plan for _, r in g if r) * N_CLIPS
     return {"value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "speedup_vs_plain": value / plain_value,
             "rd_cost_increase": loss, **work,
+            "used_option_ceiling": {"speedup_vs_plain": ceiling[0] / plain_value, "rd_cost_increase": ceiling[1],
+                                    "note": "keep words of exactly the options each superblock's exhaustive partition "
+                                            "uses (perfect predictions: the most any exact-scoring pruner of these "
+                                            "options saves at no loss), timed like the network"},
             "bd_rate": "unavailable: needs the AVM v1.0.0 encoder and decoder (not in this image)",
             "thresholds": {k: wts[k] for k in pruner.THRESHOLDS},
             "stages_ms_per_step": {k: v[0] for k, v in st.items() if v[1]},
