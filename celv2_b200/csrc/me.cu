@@ -98,6 +98,15 @@ __device__ __forceinline__ int sad8(const uint32_t* c, const DevPlane& ref, int 
   return (int)s;
 }
 
+// The 4-byte windows at p and p + 1 (any alignment) from two aligned 32-bit loads.
+__device__ __forceinline__ void load_pair(const uint8_t* p, uint32_t& lo4, uint32_t& hi4) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = (uint32_t)(a & 3) * 8, w0 = __ldg(w), w1 = __ldg(w + 1);
+  lo4 = __funnelshift_r(w0, w1, sh);
+  hi4 = __funnelshift_rc(w0, w1, sh + 8);  // a shift of 32 gives w1
+}
+
 // The refinement step's position n (raster 0..8 with the centre, 4, visited first).
 __device__ __forceinline__ int refine_pos(int t) { return t == 0 ? 4 : (t <= 4 ? t - 1 : t); }
 
@@ -378,6 +387,35 @@ __global__ void __launch_bounds__(kRefineThreads, 7) k_me_refine(const FrameJob*
 #pragma unroll
   for (int s = 0; s < 2; s++) {
     const int step = 2 - s;
+    // the half-pel step around a whole-pel MV reads four phase planes only (phase 2 one pel left
+    // or up of phase 0 at -1/2 pel, at the same pel at +1/2): the rows of the 5 x 5 footprint are
+    // loaded once per plane and the positions that share a plane take 4-byte windows of them
+    const int X = ox + (cx >> 2), Y = oy + (cy >> 2);
+    if (s == 0 && !((cx | cy) & 3) && inside(ref, X - 1, Y - 1, 5, 5)) {
+      const long long rs = ref.stride;
+      const uint8_t* p00 = ref.p + (long long)Y * rs + X;
+      uint32_t pr[5], lf[5], rt[5];
+#pragma unroll
+      for (int i = 0; i < 4; i++) pr[i] = load4(p00 + i * rs);
+      sat[0][0][t][c] = satd4_rows(C, pr);  // the centre, phase (0, 0)
+      const uint8_t* p20 = p00 + 8 * ref.phase;  // phase (2, 0): rows Y - 1 .. Y + 3
+#pragma unroll
+      for (int i = 0; i < 5; i++) pr[i] = load4(p20 + (i - 1) * rs);
+      sat[0][2][t][c] = satd4_rows(C, pr);      // (0, -1/2)
+      sat[0][7][t][c] = satd4_rows(C, pr + 1);  // (0, +1/2)
+      const uint8_t* p02 = p00 + 2 * ref.phase - 1;  // phase (0, 2): columns X - 1 .. X + 3
+#pragma unroll
+      for (int i = 0; i < 4; i++) load_pair(p02 + i * rs, lf[i], rt[i]);
+      sat[0][4][t][c] = satd4_rows(C, lf);  // (-1/2, 0)
+      sat[0][5][t][c] = satd4_rows(C, rt);  // (+1/2, 0)
+      const uint8_t* p22 = p00 + 10 * ref.phase - 1;  // phase (2, 2): both
+#pragma unroll
+      for (int i = 0; i < 5; i++) load_pair(p22 + (i - 1) * rs, lf[i], rt[i]);
+      sat[0][1][t][c] = satd4_rows(C, lf);      // (-1/2, -1/2)
+      sat[0][3][t][c] = satd4_rows(C, rt);      // (+1/2, -1/2)
+      sat[0][6][t][c] = satd4_rows(C, lf + 1);  // (-1/2, +1/2)
+      sat[0][8][t][c] = satd4_rows(C, rt + 1);  // (+1/2, +1/2)
+    } else {
 #pragma unroll
     for (int k = s; k < 9; k++) {  // the second step's centre (k = 0) is the first step's winner
       const int n = refine_pos(k);
@@ -395,6 +433,7 @@ __global__ void __launch_bounds__(kRefineThreads, 7) k_me_refine(const FrameJob*
         for (int i = 0; i < 4; i++) pr[i] = row4(ph, x, y + i);
       }
       sat[s][k][t][c] = satd4_rows(C, pr);
+    }
     }
     __syncthreads();
     // the cell's choice (me_refine: the centre first, a move must save kSubpelPenalty)
