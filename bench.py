@@ -767,7 +767,7 @@ def run_anime(args, stream_of, dist, local, cpu_1080p_s):
             loss = sum(float(v.sum()) for v in pr.values()) / sum(float(full[k].sum()) for k in pr) - 1.0
             out["pruned"] = {"frames_per_s": frames / (pms / 1e3), "speedup_vs_plain": ms / pms,
                              "rd_cost_increase": loss,
-                             "note": "the committed network (trained on 1080p sinusoid clips) on this content"}
+                             "note": "the committed network (trained on 1080p natural-like and animation-like clips) on this 4K content"}
 
         # end to end: host 10-bit planes in, records in host memory, group by group, stream by stream
         for e in engines:

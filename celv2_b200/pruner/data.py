@@ -66,12 +66,16 @@ def make_clips(seeds, frames: int = 17, workers: int = 4):
         return pool.map(_clip, [(s, frames) for s in seeds])
 
 
-def labels(words: np.ndarray, nrefs: int, pos_weight: float = 2.0):
+def labels(words: np.ndarray, nrefs: int, pos_weight: float = 2.0, regret=None, cost=None,
+           cap: float = 20.0):
     """(labels, weights), each nsb x OUTPUTS, from keep words of the used options: outputs 0..6 the
     references, 7 intra, 8..11 the levels, 12..21 intra modes 3..12 (weighed only where the chosen
     partition has intra leaves: the modes matter only when intra is kept). Absent references and
     the unused outputs weigh 0; needed options weigh `pos_weight` (missing one costs more than
-    keeping one that is not needed)."""
+    keeping one that is not needed). `regret` ({output: per superblock the cost increase of pruning
+    that option alone}) and `cost` (the exhaustive costs) scale a needed option's weight by
+    1 + regret / (the frame's mean superblock cost), at most `cap`: where the summed cost is small
+    (flat content) a missed option costs a large share of it, which the plain labels do not show."""
     words = words.astype(np.int64)
     nsb = words.size
     y = np.zeros((nsb, OUT), np.float32)
@@ -89,30 +93,70 @@ def labels(words: np.ndarray, nrefs: int, pos_weight: float = 2.0):
         y[:, MODE0 + m - 3] = (words >> (16 + m)) & 1
         w[:, MODE0 + m - 3] = has_intra
     w = np.where(y > 0, w * pos_weight, w)
+    if regret:
+        scale = max(float(np.mean(cost)), 1.0)
+        for o, reg in regret.items():
+            f = np.minimum(cap, 1.0 + np.maximum(reg.astype(np.float64), 0.0) / scale).astype(np.float32)
+            w[:, o] = np.where(y[:, o] > 0, w[:, o] * f, w[:, o])
     return y, w
 
 
-def collect(eng: E.CudaEngine, clip, qindex: int, plan=None):
+# The options whose training weight is scaled by their regret (collect(regrets=True)): output ->
+# the keep word without that option alone, for a frame of n references (None: nothing to prune --
+# a frame's only reference is always kept).
+def _without_ref(r):
+    return lambda n: None if n < 2 or r >= n else (((1 << n) - 1) & ~(1 << r)) | 0x80 | 0xF00 | 0x1FFF0000
+
+
+def _without_level(l):
+    return lambda n: ((1 << n) - 1) | 0x80 | (0xF00 & ~(0x100 << l)) | 0x1FFF0000
+
+
+REGRET_OUTPUTS = {**{r: _without_ref(r) for r in range(7)},
+                  7: lambda n: ((1 << n) - 1) | 0xF00 | 0x1FFF0000,
+                  **{8 + l: _without_level(l) for l in range(4)}}
+
+
+def collect(eng: E.CudaEngine, clip, qindex: int, plan=None, regrets: bool = False):
     """Features, labels, weights and (frame, nrefs, qindex) of every inter superblock of `clip`
     (10-bit planes, coded by `plan`) decided exhaustively, with each inter frame's exhaustive
-    superblock costs and used-option keep words."""
+    superblock costs and used-option keep words. regrets: each group is decided again once per
+    REGRET_OUTPUTS option (each reference, intra, each block level), with that option alone pruned
+    everywhere, and the cost increase per superblock scales the option's weight (labels)."""
     plan = plan or gop.mini_gop_plan(len(clip))
+    nsb = eng.sb_cols * eng.sb_rows
     eng.clear_store()
     eng.set_config(E.CFG_FEATURES, 1)
     for i, f in enumerate(clip):
         eng.upload(f, i)
     xs, ys, ws, meta, costs, used = [], [], [], [], {}, {}
     for group in plan:
-        eng.launch_group([s for s, _ in group], [r for _, r in group], qindex, to_host=True)
+        srcs, refl = [s for s, _ in group], [r for _, r in group]
+        eng.launch_group(srcs, refl, qindex, to_host=True)
+        feats, words = {}, {}
         for j, (s, refs) in enumerate(group):
-            if not refs:
-                continue
-            x = eng.features(j)
-            words = used_options(eng.group_records(j), len(refs))
-            y, w = labels(words, len(refs))
+            if refs:
+                feats[j] = eng.features(j)
+                words[j] = used_options(eng.group_records(j), len(refs))
+                costs[s] = eng.sb_costs(j)
+        reg = {j: {} for j in feats}
+        if regrets and feats:
+            for o, word in REGRET_OUTPUTS.items():
+                ks = {j: word(len(group[j][1])) for j in feats}
+                if all(k is None for k in ks.values()):
+                    continue
+                for j, k in ks.items():
+                    # a job with nothing to prune here is decided with all of it (its regret is 0)
+                    eng.set_keep(j, np.full(nsb, 0xFFFFFFFF if k is None else k, np.uint32))
+                eng.launch_group(srcs, refl, qindex)
+                for j, k in ks.items():
+                    if k is not None:
+                        reg[j][o] = eng.sb_costs(j) - costs[group[j][0]]
+        for j, x in feats.items():
+            s, refs = group[j]
+            y, w = labels(words[j], len(refs), regret=reg[j], cost=costs[s])
             xs.append(x), ys.append(y), ws.append(w)
             meta.append(np.tile([s, len(refs), qindex], (x.shape[0], 1)))
-            costs[s] = eng.sb_costs(j)
-            used[s] = words
+            used[s] = words[j]
     eng.set_config(E.CFG_FEATURES, 0)
     return (np.concatenate(xs), np.concatenate(ys), np.concatenate(ws), np.concatenate(meta)), costs, used
