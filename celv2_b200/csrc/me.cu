@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(kMeThreads, 4) k_me_level(const FrameJob* __re
 // first step's winner, whose SATD the first step has already computed.
 constexpr int kRefineCells = 32, kRefineTiles = 4, kRefineThreads = 32 * kRefineTiles;
 
-__global__ void __launch_bounds__(kRefineThreads, 7) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
+__global__ void __launch_bounds__(kRefineThreads, 8) k_me_refine(const FrameJob* __restrict__ jobs, WorkList w) {
   __shared__ int sat[2][9][kRefineTiles][kRefineCells];  // [step][position][tile][cell]
   __shared__ int unit_slot;
   const int tid = threadIdx.x, c = tid & 31, t = tid >> 5;
