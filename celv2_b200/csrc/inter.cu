@@ -258,21 +258,37 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
     //    cell's tiles are lanes l, l + 1, l + 16, l + 17 of one warp
     for (int dd = 0; dd < nc; dd += 2) {
       int sat[2];
+      const int dA = c0 + dd, dB = c0 + min(dd + 1, nc - 1);
+      if (S.mfast[dA] & S.mfast[dB]) {
+        // both MVs' rows from aligned word pairs, all 16 loads issued before either SATD
+        uint32_t wv[2][4][2];
+        uint32_t shv[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const uintptr_t a = tile_base + (uintptr_t)(intptr_t)S.moff[h ? dB : dA];
+          const uint32_t* wp = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+          shv[h] = (uint32_t)(a & 3) * 8;
+#pragma unroll
+          for (int i = 0; i < 4; i++) wv[h][i][0] = __ldg(wp + i * ws), wv[h][i][1] = __ldg(wp + i * ws + 1);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          uint32_t pr[4];
+#pragma unroll
+          for (int i = 0; i < 4; i++) pr[i] = __funnelshift_r(wv[h][i][0], wv[h][i][1], shv[h]);
+          sat[h] = satd4_rows(C, pr);
+        }
+      } else {
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const int d = c0 + min(dd + h, nc - 1);
+        const int d = h ? dB : dA;
         uint32_t pr[4];
-        if (S.mfast[d]) {  // the usual case, uniform over the CTA: rows from aligned words
+        if (S.mfast[d]) {
           const uintptr_t a = tile_base + (uintptr_t)(intptr_t)S.moff[d];
           const uint32_t* wp = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
           const uint32_t sh = (uint32_t)(a & 3) * 8;
-          if (sh == 0) {
 #pragma unroll
-            for (int i = 0; i < 4; i++) pr[i] = __ldg(wp + i * ws);
-          } else {
-#pragma unroll
-            for (int i = 0; i < 4; i++) pr[i] = __funnelshift_r(__ldg(wp + i * ws), __ldg(wp + i * ws + 1), sh);
-          }
+          for (int i = 0; i < 4; i++) pr[i] = __funnelshift_r(__ldg(wp + i * ws), __ldg(wp + i * ws + 1), sh);
         } else {
           const int m = S.D[d], mx = mv_x(m), my = mv_y(m);
           DevPlane ph = ref;
@@ -286,6 +302,7 @@ __global__ void __launch_bounds__(kInterThreads, 4) k_inter(const FrameJob* __re
           }
         }
         sat[h] = satd4_rows(C, pr);
+      }
       }
 #pragma unroll
       for (int h = 0; h < 2; h++) {
