@@ -236,6 +236,9 @@ struct celv2_engine {
   // Descriptors go to the device from a ring of pinned buffers: an asynchronous copy from pageable
   // memory may wait for the stream, which would serialise back-to-back launches.
   static constexpr int kRing = 8, kRingJobs = 2 * kMaxJobs + 1;
+  // Store slots an upload may add rather than wait for a dropped slot's readers (a caller that
+  // issues far ahead of the GPU would otherwise grow the store without bound).
+  static constexpr int kStoreSlotsIdle = 48;
   FrameJob* ring = nullptr;
   cudaEvent_t ring_done[kRing] = {};
   bool ring_pending[kRing] = {};
@@ -828,9 +831,18 @@ struct celv2_engine {
     if (key < 0) invalid("store keys must be >= 0");
     // No wait for queued work: it runs on this stream, ahead of the upload.
     Slot* s = find(key);
-    if (!s)  // a dropped store frame's memory (it has the events), the least recently used
-      for (Slot* x : store)
-        if (x->key < 0 && !x->resident && x->last_use && (!s || x->used < s->used)) s = x;
+    if (!s) {
+      // a dropped store frame's memory (it has the events): the least recently read one whose
+      // readers have all finished; with none finished, a new slot while the store holds fewer
+      // than kStoreSlotsIdle, else the least recently read one (the upload then waits for it)
+      Slot* lru = nullptr;
+      for (Slot* x : store) {
+        if (x->key >= 0 || x->resident || !x->last_use) continue;
+        if (!lru || x->used < lru->used) lru = x;
+        if ((!s || x->used < s->used) && (!x->use_pending || cudaEventQuery(x->last_use) == cudaSuccess)) s = x;
+      }
+      if (!s && (int)store.size() >= kStoreSlotsIdle) s = lru;
+    }
     if (!s) {
       s = new Slot;
       store.push_back(s);
