@@ -197,7 +197,10 @@ struct JobBuffers {
   int* intra = nullptr;      // nsb * kBlocks * kModes
   int2* inter = nullptr;     // nsb * kMaxRefs * kBlocks
   celv2_sb_out* out = nullptr;
-  celv2_sb_out* out2 = nullptr;  // group buffers: the records of every other group (see group_parity)
+  celv2_sb_out* out2 = nullptr;  // group buffers: out, out2, out3 in turn (see group_parity)
+  celv2_sb_out* out3 = nullptr;
+  // group record buffer set p (0: out, 1: out2, 2: out3)
+  celv2_sb_out* records(int p) const { return p == 0 ? out : p == 1 ? out2 : out3; }
   uint32_t* keep = nullptr;      // pruning keep words of the job, when given (nsb)
   long long* sb_cost = nullptr;  // per superblock, the chosen partition's cost (nsb)
   float* feats = nullptr;        // the learned pruner's features (nsb x CELV2_PRUNER_FEATURES)
@@ -249,12 +252,15 @@ struct celv2_engine {
   float* group_feats = nullptr;  // the group slots' pruner features, slot after slot
   celv2_sb_out* group_host = nullptr;
   int group_jobs = 0;
-  // Group records go to the host on copy_st, overlapping the next group's stages, which write the
-  // other of two device record buffers (group_parity); copied[p] marks buffer p's copies done.
+  // Group records go to the host on copy_st, overlapping the next groups' stages, which write the
+  // other device record buffers: three sets in turn (group_parity), so a group waits only for the
+  // copies of the group three back (with two, the group after a large batch waited for that
+  // batch's records to cross PCIe); copied[p] marks buffer set p's copies done.
   cudaStream_t copy_st = nullptr;
   cudaStream_t up_st = nullptr;  // celv2_upload's stream (frame-store uploads)
-  cudaEvent_t stages_done = nullptr, copied[2] = {nullptr, nullptr};
-  bool copy_pending[2] = {false, false};
+  static constexpr int kRecordSets = 3;
+  cudaEvent_t stages_done = nullptr, copied[kRecordSets] = {};
+  bool copy_pending[kRecordSets] = {};
   int group_parity = 0;
   long long kernel_launches = 0;
   // stage timing: an event pair around each stage launch, harvested when the stream is idle
@@ -374,7 +380,7 @@ struct celv2_engine {
   }
 
   static void free_buffers(JobBuffers& b) {
-    cudaFree(b.fields), cudaFree(b.intra), cudaFree(b.inter), cudaFree(b.out), cudaFree(b.out2);
+    cudaFree(b.fields), cudaFree(b.intra), cudaFree(b.inter), cudaFree(b.out), cudaFree(b.out2), cudaFree(b.out3);
     cudaFree(b.keep), cudaFree(b.sb_cost);
     if (b.owns_feats) cudaFree(b.feats);
     b = JobBuffers{};
@@ -385,7 +391,10 @@ struct celv2_engine {
     if (with_intra) CK(cudaMalloc(&b.intra, (size_t)g.nsb * kBlocks * kModes * sizeof(int)));
     CK(cudaMalloc(&b.inter, (size_t)g.nsb * kMaxRefs * kBlocks * sizeof(int2)));
     CK(cudaMalloc(&b.out, (size_t)g.nsb * sizeof(celv2_sb_out)));
-    if (with_intra) CK(cudaMalloc(&b.out2, (size_t)g.nsb * sizeof(celv2_sb_out)));
+    if (with_intra) {
+      CK(cudaMalloc(&b.out2, (size_t)g.nsb * sizeof(celv2_sb_out)));
+      CK(cudaMalloc(&b.out3, (size_t)g.nsb * sizeof(celv2_sb_out)));
+    }
     CK(cudaMalloc(&b.keep, (size_t)g.nsb * sizeof(uint32_t)));
     CK(cudaMalloc(&b.sb_cost, (size_t)g.nsb * sizeof(long long)));
     if (!with_intra) {  // the group slots' features are one block (reserve_group)
@@ -789,11 +798,11 @@ struct celv2_engine {
     return o;
   }
 
-  // The device record buffer set (0: out, 1: out2) of the next group, after `stream` waits for the
-  // host copies that still read it (two groups back).
+  // The device record buffer set (JobBuffers::records) of the next group, after `stream` waits for
+  // the host copies that still read it (kRecordSets groups back).
   int take_parity(cudaStream_t stream) {
     const int par = group_parity;
-    group_parity ^= 1;
+    group_parity = (par + 1) % kRecordSets;
     if (copy_pending[par]) {
       CK(cudaStreamWaitEvent(stream, copied[par], 0));
       copy_pending[par] = false;
@@ -921,7 +930,7 @@ struct celv2_engine {
       if (nets[j].net) jobs[j].keep = group[j].keep;
     }
     const int par = take_parity(st);
-    for (int j = 0; j < njobs; j++) jobs[j].out = par ? group[j].out2 : group[j].out;
+    for (int j = 0; j < njobs; j++) jobs[j].out = group[j].records(par);
     if (use_graphs && !timing)
       launch_graph(jobs, nets);
     else
@@ -1082,7 +1091,7 @@ void launch_multi(int njobs, celv2_engine* const* engines, const long long* src_
     en.job.keep = e->put_keep(keeps[ei][slot], e->group[slot], lead->st);
     en.net = e->net_for(en.job, e->group[slot], !keeps[ei][slot].empty());
     if (en.net.net) en.job.keep = e->group[slot].keep;
-    en.job.out = par[ei] ? e->group[slot].out2 : e->group[slot].out;
+    en.job.out = e->group[slot].records(par[ei]);
     en.e = e, en.slot = slot, en.work = (long long)(nrefs[j] + 1) * e->g.nsb, en.dest = dests[ei][slot];
     entries.push_back(en);
   }
